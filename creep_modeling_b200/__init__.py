@@ -1,0 +1,9 @@
+"""B200-native LS-EVPFFT crystal-plasticity solver (drop-in for gdebrun2/creep_modeling's lsevpfft/LS-EVPFFT).
+
+The compute path is the sm_100a library ``_build/libevp_b200.so`` (C ABI in
+``include/evp.h``); this package is the thin Python host over it.
+"""
+from .solver import Solve, run_solver, load_results, RESULTS_COLS, DIAG_COLS  # noqa: F401
+from ._lib import EvpError  # noqa: F401
+
+__all__ = ["Solve", "run_solver", "load_results", "RESULTS_COLS", "DIAG_COLS", "EvpError"]

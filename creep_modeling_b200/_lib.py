@@ -1,0 +1,85 @@
+"""ctypes binding of ``libevp_b200.so`` (the C ABI declared in ``include/evp.h``).
+
+There is no CPU fallback: if the library cannot be loaded, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_build" / "libevp_b200.so"
+
+EXPORTED = (
+    "evp_solve_file", "evp_open", "evp_advance", "evp_get_field", "evp_last_rows", "evp_stats", "evp_close",
+    "evp_last_error", "evp_version",
+)
+
+STATUS = {
+    0: "ok", -1: "deck or input-file error", -2: "deck feature not supported", -3: "singular matrix",
+    -4: "non-convergence or non-finite state", -5: "output-file error", -6: "CUDA error or no device",
+    -7: "bad argument",
+}
+
+
+class EvpError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}: {STATUS.get(code, 'error')}] {msg}")
+        self.code = code
+
+
+class Report(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("macrosteps", ctypes.c_int),
+        ("equilibrium_iters", ctypes.c_longlong),
+        ("voxel_iters", ctypes.c_longlong),
+        ("wall_s", ctypes.c_double),
+        ("gpu_s", ctypes.c_double),
+        ("n1", ctypes.c_int),
+        ("n2", ctypes.c_int),
+        ("n3", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load(path: Path | str | None = None):
+    """Load the library (building it first when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        from . import build as _build
+
+        _build.build()
+    L = ctypes.CDLL(str(p))
+    c_dp = ctypes.POINTER(ctypes.c_double)
+    vp = ctypes.c_void_p
+    L.evp_solve_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(Report)]
+    L.evp_solve_file.restype = ctypes.c_int
+    L.evp_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.evp_open.restype = ctypes.c_int
+    L.evp_advance.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.evp_advance.restype = ctypes.c_int
+    L.evp_get_field.argtypes = [vp, ctypes.c_char_p, c_dp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    L.evp_get_field.restype = ctypes.c_int
+    L.evp_last_rows.argtypes = [vp, c_dp, c_dp]
+    L.evp_last_rows.restype = ctypes.c_int
+    L.evp_stats.argtypes = [vp, ctypes.POINTER(Report)]
+    L.evp_stats.restype = ctypes.c_int
+    L.evp_close.argtypes = [vp]
+    L.evp_close.restype = ctypes.c_int
+    L.evp_last_error.argtypes = []
+    L.evp_last_error.restype = ctypes.c_char_p
+    L.evp_version.argtypes = []
+    L.evp_version.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise EvpError(rc, (load().evp_last_error() or b"").decode())

@@ -1,0 +1,137 @@
+// evp_dev.cuh -- device-resident state of one LS-EVPFFT solve and kernel entry points.
+//
+// HBM layout: structure of arrays, FP64, one contiguous array per field with
+// the component index outermost: field[c * N + v], voxel v = i + n1*(j + n2*k).
+// Symmetric tensors are stored as s6 = (11,22,33,23,13,12); full 3x3 tensors
+// row-major (c = 3*row + col); 6x6 operators row-major (c = 6*row + col).
+// The half spectrum of the FFT work array is complex128
+// spec[c][k][j][kx], kx in [0, n1/2].
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace evp {
+
+constexpr int kMaxSysDev = 24;
+
+// Per-phase constants (phase_type, types.f90:96-118) in device memory.
+struct PhaseDev {
+    int nsyst, nmodes, igas, int_exp;  // int_exp: every nrs-1 is an integer in [0,64]
+    int nsm[3];
+    double nrs[kMaxSysDev], gamd0[kMaxSysDev], hpfac[kMaxSysDev];
+    double tau0f[kMaxSysDev], tau0b[kMaxSysDev];
+    double tau1[3], thet0[3], thet1[3];  // per mode, from its last system (harden, various_functions.f90:1466-1470)
+    double hard[kMaxSysDev * kMaxSysDev];
+    double dnca[kMaxSysDev * 3], dbca[kMaxSysDev * 3];
+    double C[81];
+};
+
+// Offsets (in doubles) of the per-kernel results in the small result buffer.
+enum : int {
+    OFF_SGAVG = 0,    // 6   sum wgtc*sg over all voxels
+    OFF_DU = 8,       // 9   BC correction of the average velgrad (reference config)
+    OFF_CORR = 24,    // 31  sum velgrad*wgtc (all, gas, solid), dL mixing sums
+    OFF_NEWTON = 64,  // 14  errs, erre, sum wgtc*sg (solid), sum wgtc*sg (all)
+    OFF_INIT = 80,    // 36  sum cg66*wgtc (solid)
+    OFF_UPD1 = 120,   // 40  F averages, weights, max solid vm rate
+    OFF_DU2 = 160,    // 9   average-velgrad fix of update_tensor_config
+    OFF_UPD3 = 176,   // 30+13 averages, hardening sums, last solid voxel
+    OFF_DIAG = 224,   // 24+ diagnostics reductions
+    OFF_C0 = 272,     // 117 macro tangent sums
+    OFF_KIN = 392,    // 4   kinematic increment maxima
+    OFF_DC = 400,     // 18  DC of the grid-update spectrum (complex x 9)
+    OFF_G0 = 420,     // 81  real-space Green operator at the origin
+    RED_OUT_SIZE = 512
+};
+
+enum : int { CNT_SGAVG = 0, CNT_XINV, CNT_CORR, CNT_NEWTON, CNT_INIT, CNT_UPD1, CNT_UPD2, CNT_UPD3, CNT_DIAG, CNT_DIAG2, CNT_C0, CNT_KIN, CNT_G0, CNT_N };
+
+struct FftPlan1D {
+    int n;
+    int nst;
+    int rad[8];
+};
+
+struct Dev {
+    long long N;
+    int n1, n2, n3, n1h, n3node;
+    int nsys;  // max nsyst over phases (array stride of the per-system fields)
+    int grid;  // blocks of the voxel kernels
+    double wgt;
+    // voxel state
+    double *sg, *sgt, *edotp, *ept, *disgradsym;         // s6
+    double *velgrad, *velgradold, *dvr;                  // 9
+    double *F, *Finv, *Fe, *Fp, *Finc, *Feinc, *ag;      // 9
+    double *detF, *wgtc, *epvm, *gacumgr;                // 1
+    double *sg66, *c066mod, *cG, *cgas;                  // 36 (cG, cgas may be null)
+    double *sch;                                         // 5*nsys   [(s*5+c)*N + v]
+    double *crss, *trialtau;                             // 2*nsys   [(s*2+c)*N + v]
+    double *gamdot;                                      // nsys
+    double *eth;                                         // 9 or null
+    uint8_t *gas, *phase;                                // phase index 0-based
+    // snapshot copies (take_snapshot / rollback)
+    double *s_velgrad, *s_velgradold, *s_sg, *s_edotp, *s_gamdot, *s_trialtau;
+    // spectrum, twiddles, grid-update scratch
+    double2 *spec;
+    double2 *tw1, *tw2, *tw3;
+    double *dv3, *xnode;
+    // reductions
+    double *partials, *red;
+    unsigned int *counters;
+    int *err;  // error word: bit 0 singular matrix, bit 1 non-finite Newton result
+    const PhaseDev *ph;
+    int nph;
+};
+
+struct CorrParams {
+    double mix, Lscale;
+    int do_mix, kinematic;
+};
+struct NewtonParams {
+    double tdot, error, erroral, complgas;
+    int modal, thermo, iuphard;
+};
+struct XinvParams {
+    double dvelgradavg[9];
+    double dinv[9];  // inverse of the average F^{-1} (current config)
+};
+struct Upd1Params {
+    double tdot;
+    int iupdate;
+};
+struct Upd2Params {
+    double velgradavg[9];
+};
+struct Upd3Params {
+    double tdot;
+    int iupdate, iuphard;
+    long long vlast;  // last solid voxel in loop order (for the eelav quirk, LS-EVPFFT.f90:482-483)
+};
+
+// ---- launch wrappers (stream-ordered)
+void launch_init(const Dev& d, const double* euler, const int* grain, const double* hp, const double* udot9, const double* u6t,
+                 cudaStream_t st);
+void launch_sgavg(const Dev& d, cudaStream_t st);
+void launch_prologue(const Dev& d, const double* c0, const double* goperr0, int do_schmid, int modal, cudaStream_t st);
+void launch_goperr0(const Dev& d, const double* c0, const double* s0, cudaStream_t st);
+void launch_gas_compl(const Dev& d, double tdot, double complgas, int modal, cudaStream_t st);
+void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st);
+void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st);
+void launch_upd1(const Dev& d, const Upd1Params& p, cudaStream_t st);
+void launch_upd2(const Dev& d, const Upd2Params& p, cudaStream_t st);
+void launch_upd3(const Dev& d, const Upd3Params& p, cudaStream_t st);
+void launch_diag(const Dev& d, double Lfloor, cudaStream_t st);
+void launch_c0(const Dev& d, double tdot, double tdotref, cudaStream_t st);
+void launch_kinematic(const Dev& d, double tdot_step, cudaStream_t st);
+void launch_cell2node(const Dev& d, double tdot, int ideriv, cudaStream_t st);
+
+// FFT engine (evp_fft.cu)
+FftPlan1D make_plan(int n);
+void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st);
+void fft_configure();
+void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st);
+void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st);
+void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st);
+void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st);
+
+}  // namespace evp

@@ -1,0 +1,569 @@
+// evp_fft.cu -- FP64 3-D FFT engine of the spectral equilibrium step.
+//
+// Replaces the FFTW C2C plans of fourier_functions.f90:69-336 (forward of the
+// 9 PK1 fields, Green-operator product, inverse, real part / N) with a
+// half-spectrum transform in five passes over HBM:
+//   x: R2C by packing two voxel rows into one complex pencil (prologue computes
+//      P' = J (sigma - <sigma>) F^{-T}, LS-EVPFFT.f90:256-269, in registers)
+//   y: C2C
+//   z: C2C forward -> Gamma(xi):P'(xi) evaluated on the fly from c0
+//      (form_G igamma=0 + convolution_with_Goper, various_functions.f90:640-809,
+//      999-1037) -> C2C inverse, one kernel, one read + one write of the spectrum
+//   y: C2C inverse
+//   x: C2R + epilogue (dvelgradref, and the F^{-1}-weighted average that
+//      correction_to_current needs, various_functions.f90:1085-1101)
+// Each pass stages pencils in shared memory and runs a mixed-radix Stockham
+// FFT (radices 2,3,4,5,7,8,11,13) with twiddles from a per-axis table.
+// The grid-update path (integrate_tensor2, various_functions.f90:359-429) reuses
+// the same passes with a different z operator.
+#include "evp_dev.cuh"
+#include "evp_math.cuh"
+
+#include <stdexcept>
+#include <string>
+
+namespace evp {
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 mul_mi(double2 a) { return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_small(double2 (&v)[R], const double2* __restrict__ tw, int n) {
+    if constexpr (R == 2) {
+        double2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]), t3 = mul_mi<INV>(csub(v[1], v[3]));
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    } else if constexpr (R == 8) {
+        const double c = 0.70710678118654752440;
+        double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<4, INV>(e, tw, n);
+        dft_small<4, INV>(o, tw, n);
+        double2 w1 = INV ? make_double2(c, c) : make_double2(c, -c);
+        double2 w3 = INV ? make_double2(-c, c) : make_double2(-c, -c);
+        double2 p0 = o[0], p1 = cmul(o[1], w1), p2 = mul_mi<INV>(o[2]), p3 = cmul(o[3], w3);
+        v[0] = cadd(e[0], p0); v[4] = csub(e[0], p0);
+        v[1] = cadd(e[1], p1); v[5] = csub(e[1], p1);
+        v[2] = cadd(e[2], p2); v[6] = csub(e[2], p2);
+        v[3] = cadd(e[3], p3); v[7] = csub(e[3], p3);
+    } else {
+        double2 in[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) in[r] = v[r];
+        const int step = n / R;
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            double2 acc = in[0];
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                double2 w = tw[((r * q) % R) * step];
+                if (INV) w.y = -w.y;
+                acc = cadd(acc, cmul(in[r], w));
+            }
+            v[q] = acc;
+        }
+    }
+}
+
+// One Stockham stage over P pencils of length n stored element-major in
+// shared memory: element e of pencil p at s[e*ES + p].
+template <int R, bool INV>
+__device__ __forceinline__ void fft_stage(double2* s, int ES, int P, int n, int Ns, const double2* __restrict__ tw) {
+    constexpr int MAXB = 4;
+    const int nb = n / R, total = nb * P;
+    double2 v[MAXB][R];
+#pragma unroll
+    for (int q = 0; q < MAXB; q++) {
+        const int b = threadIdx.x + q * blockDim.x;
+        if (b < total) {
+            const int p = b % P, j = b / P;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[q][r] = s[(j + r * nb) * ES + p];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < MAXB; q++) {
+        const int b = threadIdx.x + q * blockDim.x;
+        if (b < total) {
+            const int p = b % P, j = b / P, jm = j % Ns;
+            const int step = jm * (n / (Ns * R));
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                double2 w = tw[r * step];
+                if (INV) w.y = -w.y;
+                v[q][r] = cmul(v[q][r], w);
+            }
+            dft_small<R, INV>(v[q], tw, n);
+            const int idxD = (j / Ns) * Ns * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; r++) s[(idxD + r * Ns) * ES + p] = v[q][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <bool INV>
+__device__ void fft_run(double2* s, int ES, int P, const FftPlan1D& pl, const double2* __restrict__ tw) {
+    int Ns = 1;
+    for (int st = 0; st < pl.nst; st++) {
+        const int R = pl.rad[st];
+        switch (R) {
+            case 2: fft_stage<2, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 3: fft_stage<3, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 4: fft_stage<4, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 5: fft_stage<5, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 7: fft_stage<7, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 8: fft_stage<8, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 11: fft_stage<11, INV>(s, ES, P, pl.n, Ns, tw); break;
+            case 13: fft_stage<13, INV>(s, ES, P, pl.n, Ns, tw); break;
+            default: break;
+        }
+        Ns *= R;
+    }
+}
+
+FftPlan1D make_plan(int n) {
+    FftPlan1D pl;
+    pl.n = n;
+    pl.nst = 0;
+    int m = n, e2 = 0;
+    while (m % 2 == 0) { m /= 2; e2++; }
+    // powers of two: as many radix-8 as possible, a lone factor 2 turned into 4*4
+    int n8 = e2 / 3, rem = e2 % 3, n4 = 0, n2 = 0;
+    if (rem == 2) n4 = 1;
+    else if (rem == 1) {
+        if (n8 > 0) { n8--; n4 = 2; }
+        else n2 = 1;
+    }
+    for (int i = 0; i < n8; i++) pl.rad[pl.nst++] = 8;
+    for (int i = 0; i < n4; i++) pl.rad[pl.nst++] = 4;
+    for (int i = 0; i < n2; i++) pl.rad[pl.nst++] = 2;
+    const int odd[5] = {3, 5, 7, 11, 13};
+    for (int f : odd)
+        while (m % f == 0) {
+            if (pl.nst >= 8) throw std::runtime_error("FFT length has too many factors: " + std::to_string(n));
+            pl.rad[pl.nst++] = f;
+            m /= f;
+        }
+    if (m != 1) throw std::runtime_error("unsupported FFT length " + std::to_string(n) + " (prime factors must be <= 13)");
+    return pl;
+}
+static int min_radix(const FftPlan1D& pl) {
+    int r = 64;
+    for (int i = 0; i < pl.nst; i++) r = pl.rad[i] < r ? pl.rad[i] : r;
+    return pl.nst ? r : 1;
+}
+static int pick_threads(int P, const FftPlan1D& pl, int want) {
+    const int need = (P * pl.n / min_radix(pl) + 3) / 4;
+    int t = want > need ? want : need;
+    t = (t + 31) / 32 * 32;
+    if (t > 1024) throw std::runtime_error("FFT tile too large");
+    return t;
+}
+
+// ---------------------------------------------------------------- x forward (R2C)
+// mode 0: P'_ij = J * ((sigma - <sigma>) F^{-T})_ij ; mode 1: (L F)_ij (grid update)
+__global__ void k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
+    extern __shared__ double2 s[];
+    const int n1 = d.n1, n1h = d.n1h;
+    const long long N = d.N;
+    const int nrows = d.n2 * d.n3;
+    const int P = 9 * G;
+    const int pair0 = blockIdx.x * G;
+    __shared__ double sga[6];
+    if (mode == 0 && threadIdx.x < 6) sga[threadIdx.x] = __ldcg(&d.red[sg_off + threadIdx.x]);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < G * 2 * n1; idx += blockDim.x) {
+        const int g = idx / (2 * n1), rem = idx % (2 * n1), half = rem / n1, x = rem % n1;
+        const int row = 2 * (pair0 + g) + half;
+        double val[9];
+        if (row < nrows) {
+            const long long v = (long long)row * n1 + x;
+            if (mode == 0) {
+                double sig[9], fi[9], a6[6];
+#pragma unroll
+                for (int c = 0; c < 6; c++) a6[c] = d.sg[c * N + v] - sga[c];
+                s6_to_t2(a6, sig);
+#pragma unroll
+                for (int c = 0; c < 9; c++) fi[c] = d.Finv[c * N + v];
+                const double J = d.detF[v];
+                mm3_bt(sig, fi, val);
+#pragma unroll
+                for (int c = 0; c < 9; c++) val[c] = val[c] * J;
+            } else {
+                double L[9], F[9];
+#pragma unroll
+                for (int c = 0; c < 9; c++) { L[c] = d.velgrad[c * N + v]; F[c] = d.F[c * N + v]; }
+                mm3(L, F, val);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 9; c++) val[c] = 0.0;
+        }
+        double* sd = reinterpret_cast<double*>(s);
+#pragma unroll
+        for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = val[c];
+    }
+    __syncthreads();
+    fft_run<false>(s, P, P, pl, d.tw1);
+    // unpack the two real rows of every pencil
+    for (int idx = threadIdx.x; idx < P * n1h; idx += blockDim.x) {
+        const int k = idx % n1h, p = idx / n1h;
+        const int c = p / G, g = p % G;
+        const double2 Z = s[k * P + p];
+        const double2 Zc = cconj(s[((n1 - k) % n1) * P + p]);
+        const double2 Xa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+        const double2 dZ = csub(Z, Zc);
+        const double2 Xb = make_double2(0.5 * dZ.y, -0.5 * dZ.x);
+        const int ra = 2 * (pair0 + g);
+        if (ra < nrows) d.spec[((long long)c * nrows + ra) * n1h + k] = Xa;
+        if (ra + 1 < nrows) d.spec[((long long)c * nrows + ra + 1) * n1h + k] = Xb;
+    }
+}
+
+// ---------------------------------------------------------------- y (C2C)
+template <bool INV>
+__global__ void k_fft_y(Dev d, FftPlan1D pl, int T) {
+    extern __shared__ double2 s[];
+    const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
+    const int kx0 = blockIdx.x * T, k3 = blockIdx.y, c = blockIdx.z;
+    double2* base = d.spec + ((long long)c * n3 + k3) * n2 * n1h;
+    for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
+        const int t = idx % T, j = idx / T, kx = kx0 + t;
+        s[j * T + t] = (kx < n1h) ? base[(long long)j * n1h + kx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    fft_run<INV>(s, T, T, pl, d.tw2);
+    for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
+        const int t = idx % T, j = idx / T, kx = kx0 + t;
+        if (kx < n1h) base[(long long)j * n1h + kx] = s[j * T + t];
+    }
+}
+
+// ---------------------------------------------------------------- z fused with the Green operator
+__device__ __forceinline__ double xi_of(int k, int n) {
+    const double twopi = 2.0 * EVP_PI;
+    return (k + 1 <= n / 2) ? twopi * (double)k / (double)n : twopi * (double)(k - n) / (double)n;
+}
+
+__global__ void k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
+    extern __shared__ double2 s[];
+    __shared__ double c0[81], s0[81];
+    const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
+    const int kx0 = blockIdx.x * T, j = blockIdx.y;
+    const int P = 9 * T;
+    for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = c0g[i]; s0[i] = s0g[i]; }
+    const long long plane = (long long)n2 * n1h;
+    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+        s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    fft_run<false>(s, P, P, pl, d.tw3);
+    const bool nyq_y = (n2 % 2 == 0 && j == n2 / 2);
+    const double xiy = xi_of(j, n2);
+    for (int idx = threadIdx.x; idx < T * n3; idx += blockDim.x) {
+        const int t = idx % T, k3 = idx / T, kx = kx0 + t;
+        if (kx >= n1h) continue;
+        double2* q = s + k3 * P + t;
+        double2 a[9], r[9];
+#pragma unroll
+        for (int c = 0; c < 9; c++) a[c] = q[c * T];
+        const bool nyq = (n1 % 2 == 0 && kx == n1 / 2) || nyq_y || (n3 % 2 == 0 && k3 == n3 / 2 && n3 > 1);
+        if (kx == 0 && j == 0 && k3 == 0) {
+#pragma unroll
+            for (int c = 0; c < 9; c++) r[c] = make_double2(0.0, 0.0);
+        } else if (nyq) {
+            // Nyquist planes: Gamma = -s0 (various_functions.f90:646-651)
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int e = 0; e < 9; e++) {
+                    const double g = -s0[c * 9 + e];
+                    acc.x += g * a[e].x;
+                    acc.y += g * a[e].y;
+                }
+                r[c] = acc;
+            }
+        } else {
+            const double xi[3] = {xi_of(kx, n1), xiy, (n3 == 1) ? 0.0 : xi_of(k3, n3)};
+            double A[9], ai[9];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    double x = 0.0;
+#pragma unroll
+                    for (int jj = 0; jj < 3; jj++)
+#pragma unroll
+                        for (int l = 0; l < 3; l++) x += c0[((i * 3 + jj) * 3 + k) * 3 + l] * (xi[jj] * xi[l]);
+                    A[3 * i + k] = x;
+                }
+            if (inv3(A, ai) != 0) atomicOr(d.err, 1);
+            // r_ij = -xi_j * sum_k ai_ik (P xi)_k
+            double2 pv[3], wv[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < 3; l++) { acc.x += a[3 * k + l].x * xi[l]; acc.y += a[3 * k + l].y * xi[l]; }
+                pv[k] = acc;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int k = 0; k < 3; k++) { acc.x += ai[3 * i + k] * pv[k].x; acc.y += ai[3 * i + k] * pv[k].y; }
+                wv[i] = acc;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) r[3 * i + jj] = make_double2(-xi[jj] * wv[i].x, -xi[jj] * wv[i].y);
+        }
+#pragma unroll
+        for (int c = 0; c < 9; c++) q[c * T] = r[c];
+    }
+    __syncthreads();
+    fft_run<true>(s, P, P, pl, d.tw3);
+    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+        if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
+    }
+}
+
+// ---------------------------------------------------------------- z fused with the spectral integration (grid update)
+__global__ void k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
+    extern __shared__ double2 s[];
+    const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
+    const int kx0 = blockIdx.x * T, j = blockIdx.y;
+    const int P = 9 * T;
+    const long long plane = (long long)n2 * n1h;
+    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+        s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    fft_run<false>(s, P, P, pl, d.tw3);
+    if (blockIdx.x == 0 && j == 0 && threadIdx.x < 9) {
+        const double2 z = s[threadIdx.x * T];
+        d.red[OFF_DC + 2 * threadIdx.x] = z.x;
+        d.red[OFF_DC + 2 * threadIdx.x + 1] = z.y;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < T * n3; idx += blockDim.x) {
+        const int t = idx % T, k3 = idx / T, kx = kx0 + t;
+        if (kx >= n1h) continue;
+        double2* q = s + k3 * P + t;
+        double2 g[9];
+#pragma unroll
+        for (int c = 0; c < 9; c++) g[c] = q[c * T];
+        const double xi[3] = {xi_of(kx, n1), xi_of(j, n2), (n3 == 1) ? 0.0 : xi_of(k3, n3)};
+        double2 km[3];
+        if (ideriv == 2) {
+            // kmod = i/4 (1+e^{i xi1})(1+e^{i xi2})(1+e^{i xi3}) * tan(xi/2)
+            double2 b = make_double2(0.0, 0.25);
+            for (int l = 0; l < 3; l++) {
+                double sn, cs;
+                sincos(xi[l], &sn, &cs);
+                b = cmul(b, make_double2(1.0 + cs, sn));
+            }
+            for (int l = 0; l < 3; l++) { const double tn = tan(xi[l] / 2.0); km[l] = make_double2(tn * b.x, tn * b.y); }
+        } else {
+            for (int l = 0; l < 3; l++) km[l] = make_double2(0.0, (ideriv == 0) ? xi[l] : sin(xi[l]));
+        }
+        const double kk = km[0].x * km[0].x + km[0].y * km[0].y + km[1].x * km[1].x + km[1].y * km[1].y + km[2].x * km[2].x +
+                          km[2].y * km[2].y;
+        double2 u[3];
+        for (int l = 0; l < 3; l++) {
+            double2 acc = make_double2(0.0, 0.0);
+            if (kk > 0.0)
+                for (int m = 0; m < 3; m++) {
+                    const double2 t2 = cmul(cconj(km[m]), g[3 * l + m]);
+                    acc = cadd(acc, make_double2(t2.x / kk, t2.y / kk));
+                }
+            u[l] = acc;
+        }
+        if (ideriv == 2 && (n1 % 2 == 0 && kx == n1 / 2) && (n2 % 2 == 0 && j == n2 / 2) && (n3 % 2 == 0 && k3 == n3 / 2 && n3 > 1))
+            for (int l = 0; l < 3; l++) u[l] = make_double2(0.0, 0.0);
+        for (int l = 0; l < 3; l++) q[l * T] = u[l];
+    }
+    __syncthreads();
+    fft_run<true>(s, P, 3 * T, pl, d.tw3);
+    for (int idx = threadIdx.x; idx < 3 * T * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 3, k3 = r / 3, kx = kx0 + t;
+        if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
+    }
+}
+
+// ---------------------------------------------------------------- x inverse (C2R)
+__global__ void k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
+    extern __shared__ double2 s[];
+    const int n1 = d.n1, n1h = d.n1h;
+    const long long N = d.N;
+    const int nrows = d.n2 * d.n3;
+    const int P = ncomp * G;
+    const int pair0 = blockIdx.x * G;
+    const bool even = (n1 % 2 == 0);
+    for (int idx = threadIdx.x; idx < P * n1; idx += blockDim.x) {
+        const int x = idx % n1, p = idx / n1;
+        const int c = p / G, g = p % G;
+        const int ra = 2 * (pair0 + g);
+        const int k = (x <= n1 / 2) ? x : n1 - x;
+        const bool cj = (x > n1 / 2);
+        double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+        if (ra < nrows) A = d.spec[((long long)c * nrows + ra) * n1h + k];
+        if (ra + 1 < nrows) B = d.spec[((long long)c * nrows + ra + 1) * n1h + k];
+        if (k == 0 || (even && k == n1 / 2)) { A.y = 0.0; B.y = 0.0; }
+        if (cj) { A.y = -A.y; B.y = -B.y; }
+        s[x * P + p] = make_double2(A.x - B.y, A.y + B.x);
+    }
+    __syncthreads();
+    fft_run<true>(s, P, P, pl, d.tw1);
+    const double invN = 1.0 / (double)N;
+    double acc[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) acc[c] = 0.0;
+    for (int idx = threadIdx.x; idx < G * 2 * n1; idx += blockDim.x) {
+        const int g = idx / (2 * n1), rem = idx % (2 * n1), half = rem / n1, x = rem % n1;
+        const int row = 2 * (pair0 + g) + half;
+        if (row >= nrows) continue;
+        const long long v = (long long)row * n1 + x;
+        const double* sd = reinterpret_cast<const double*>(s);
+        if (mode == 0) {
+            double t[9], fi[9], u[9];
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                t[c] = sd[2 * (x * P + c * G + g) + half] / (double)N;
+                d.dvr[c * N + v] = t[c];
+                fi[c] = d.Finv[c * N + v];
+            }
+            mm3(t, fi, u);
+            const double w = d.wgtc[v];
+#pragma unroll
+            for (int c = 0; c < 9; c++) acc[c] += w * u[c];
+        } else {
+            for (int c = 0; c < ncomp; c++) d.dv3[c * N + v] = sd[2 * (x * P + c * G + g) + half] / (double)N;
+        }
+    }
+    (void)invN;
+    if (mode != 0) return;
+    // block partials -> the last block forms du = (dvelgradavg - <dL_ref F^{-1}>) inv(<F^{-1}>)
+    __shared__ double sh[9][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int f = 0; f < 9; f++) {
+        double x = acc[f];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[f][warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int f = 0; f < 9; f++) {
+            double x = lane < nw ? sh[f][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) d.partials[(size_t)blockIdx.x * 9 + f] = x;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(d.counters + CNT_XINV, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double fl[9], dd[9], du[9];
+        for (int f = 0; f < 9; f++) {
+            double x = 0.0;
+            for (unsigned b = 0; b < gridDim.x; b++) x += __ldcg(&d.partials[(size_t)b * 9 + f]);
+            fl[f] = x;
+            dd[f] = xp.dvelgradavg[f] - fl[f];
+        }
+        mm3(dd, xp.dinv, du);
+        for (int f = 0; f < 9; f++) d.red[OFF_DU + f] = du[f];
+        d.counters[CNT_XINV] = 0;
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+static int x_rows_per_block(int n1) { return (256 / n1) > 1 ? 256 / n1 : 1; }
+
+void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
+    const int G = x_rows_per_block(d.n1);
+    const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
+    const int grid = (npairs + G - 1) / G;
+    const int P = 9 * G;
+    const int thr = pick_threads(P, pl, 256);
+    const size_t smem = (size_t)P * d.n1 * sizeof(double2);
+    k_fft_x_fwd<<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
+}
+
+static int y_tile(const Dev& d) {
+    const int budget = 40 * 1024;
+    int nt = (int)(((long long)d.n1h * d.n2 * 16 + budget - 1) / budget);
+    if (nt < 1) nt = 1;
+    return (d.n1h + nt - 1) / nt;
+}
+void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
+    const int T = y_tile(d);
+    dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
+    const int thr = pick_threads(T, pl, 128);
+    const size_t smem = (size_t)T * d.n2 * sizeof(double2);
+    if (inverse) k_fft_y<true><<<grid, thr, smem, st>>>(d, pl, T);
+    else k_fft_y<false><<<grid, thr, smem, st>>>(d, pl, T);
+}
+
+static int z_tile(const Dev& d) {
+    const int budget = 72 * 1024;
+    int nt = (int)(((long long)d.n1h * 9 * d.n3 * 16 + budget - 1) / budget);
+    if (nt < 1) nt = 1;
+    return (d.n1h + nt - 1) / nt;
+}
+void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
+    const int T = z_tile(d);
+    dim3 grid((d.n1h + T - 1) / T, d.n2);
+    const int thr = pick_threads(9 * T, pl, 256);
+    const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
+    k_fft_z_green<<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
+}
+void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
+    const int T = z_tile(d);
+    dim3 grid((d.n1h + T - 1) / T, d.n2);
+    const int thr = pick_threads(9 * T, pl, 256);
+    const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
+    k_fft_z_integ<<<grid, thr, smem, st>>>(d, pl, T, ideriv);
+}
+void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
+    const int G = x_rows_per_block(d.n1);
+    const int ncomp = (mode == 0) ? 9 : 3;
+    const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
+    const int grid = (npairs + G - 1) / G;
+    const int P = ncomp * G;
+    const int thr = pick_threads(P, pl, 256);
+    const size_t smem = (size_t)P * d.n1 * sizeof(double2);
+    k_fft_x_inv<<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
+}
+
+// Raise the dynamic shared-memory limit of the FFT kernels (once per process).
+void fft_configure() {
+    cudaFuncSetAttribute(k_fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_fft_z_integ, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+}
+
+}  // namespace evp

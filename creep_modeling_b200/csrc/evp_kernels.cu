@@ -1,0 +1,1187 @@
+// evp_kernels.cu -- per-voxel sm_100a kernels of the LS-EVPFFT solve.
+//
+// One thread per voxel (grid-stride), SoA FP64 state (layout in evp_dev.cuh).
+// Every reduction is a fixed-order tree: warp shuffles, one partial per block,
+// and the last block to finish sums the partials in block order, so results
+// are reproducible run to run.  Kernel <-> reference routine map:
+//   k_init      data_grain + Hall-Petch init + initial_guess (IO_functions.f90:722-812, 107-199;
+//               various_functions.f90:8-53) and the start-up c066 sum (LS-EVPFFT.f90:156-165)
+//   k_sgavg     stress average before the PK1 prologue (LS-EVPFFT.f90:238-254)
+//   k_prologue  update_schmid + calc_c066mod_Goperr066mod (various_functions.f90:472-539, 812-906)
+//   k_gas_compl calc_gas_compl (various_functions.f90:909-951)
+//   k_corr      correction_to_current pass 2 + velgrad mixing (various_functions.f90:1103-1139;
+//               LS-EVPFFT.f90:277-311)
+//   k_newton    solve_res / plastic_strain_rate / elastic_strain_rate / harden
+//               (various_functions.f90:1142-1491) + the stress sums of calc_velgradavg_corr (1556-1578)
+//   k_upd1      accepted-step commit (LS-EVPFFT.f90:432-446) + update_plastic_defgrad + update_defgrad
+//   k_upd2      update_elstic_defgrad + update_el_stiff + update_tensor_config pass 1
+//   k_upd3      update_tensor_config pass 2 + update_hardening + macro averages (LS-EVPFFT.f90:460-523)
+//   k_diag      update_diagnostics (types.f90:345-692)
+//   k_c0        calc_c0 voxel part (various_functions.f90:2537-2634)
+//   k_kinematic kinematic_increments (various_functions.f90:2766-2837)
+//   k_goperr0   real-space Green operator at the origin (various_functions.f90:798-807)
+//   k_cell2node cell2node_tensor1 + nodal update (various_functions.f90:2026-2054, 2652-2691)
+#include "evp_dev.cuh"
+#include "evp_math.cuh"
+
+#include <cstdio>
+
+namespace evp {
+
+constexpr int kBlock = 256;
+constexpr int kNewtonBlock = 128;
+
+// ---------------------------------------------------------------- reductions
+// NS sums then NM maxima per thread -> one partial per block -> the last block
+// finishing folds the partials in block order into out[0 .. NS+NM).
+template <int NS, int NM>
+__device__ void reduce_store(const double* sums, const double* maxs, double* partials, double* out, unsigned int* counter) {
+    constexpr int NF = NS + NM;
+    __shared__ double sh[NF][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        double x = (f < NS) ? sums[f] : maxs[f - NS];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double y = __shfl_down_sync(0xffffffffu, x, o);
+            x = (f < NS) ? x + y : fmax(x, y);
+        }
+        if (lane == 0) sh[f][warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int f = 0; f < NF; f++) {
+            double x = (lane < nw) ? sh[f][lane] : ((f < NS) ? 0.0 : -EVP_HUGE);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                double y = __shfl_down_sync(0xffffffffu, x, o);
+                x = (f < NS) ? x + y : fmax(x, y);
+            }
+            if (lane == 0) partials[(size_t)blockIdx.x * NF + f] = x;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        for (int f = threadIdx.x; f < NF; f += blockDim.x) {
+            double s = (f < NS) ? 0.0 : -EVP_HUGE;
+            for (unsigned b = 0; b < gridDim.x; b++) {
+                double y = __ldcg(&partials[(size_t)b * NF + f]);
+                s = (f < NS) ? s + y : fmax(s, y);
+            }
+            out[f] = s;
+        }
+        if (threadIdx.x == 0) *counter = 0;
+    }
+}
+
+__device__ __forceinline__ void set_err(int* err, int bit) { atomicOr(err, bit); }
+
+__device__ __forceinline__ void ld9(const double* __restrict__ a, long long N, long long v, double* o) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) o[c] = a[c * N + v];
+}
+__device__ __forceinline__ void st9(double* __restrict__ a, long long N, long long v, const double* o) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) a[c * N + v] = o[c];
+}
+__device__ __forceinline__ void ld6(const double* __restrict__ a, long long N, long long v, double* o) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) o[c] = a[c * N + v];
+}
+__device__ __forceinline__ void st6(double* __restrict__ a, long long N, long long v, const double* o) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) a[c * N + v] = o[c];
+}
+__device__ __forceinline__ void eye9(double* a) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) a[c] = (c % 4 == 0) ? 1.0 : 0.0;
+}
+
+// |x|^e for the power law: integer exponents by binary powering, else pow().
+__device__ __forceinline__ double powabs(double x, double e, int int_exp) {
+    double a = fabs(x);
+    if (int_exp) {
+        int k = (int)e;
+        double r = 1.0, b = a;
+        while (k) {
+            if (k & 1) r *= b;
+            b *= b;
+            k >>= 1;
+        }
+        return r;
+    }
+    return pow(a, e);
+}
+
+// ---------------------------------------------------------------- k_init
+struct InitParams {
+    double udot[9];
+    double u6t[6];  // b6(udot) * tdot of process 1
+};
+
+__global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict__ euler, const int* __restrict__ grain,
+                                                   const double* __restrict__ hp, InitParams ip) {
+    const long long N = d.N;
+    double sums[36];
+#pragma unroll
+    for (int c = 0; c < 36; c++) sums[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const int p = d.phase[v];
+        const PhaseDev& ph = d.ph[p];
+        double I9[9];
+        eye9(I9);
+        st9(d.F, N, v, I9); st9(d.Fe, N, v, I9); st9(d.Fp, N, v, I9); st9(d.Finv, N, v, I9);
+        st9(d.Finc, N, v, I9); st9(d.Feinc, N, v, I9);
+        d.detF[v] = 1.0;
+        d.wgtc[v] = d.wgt;
+        d.epvm[v] = 0.0;
+        d.gacumgr[v] = 0.0;
+        st9(d.velgrad, N, v, ip.udot);
+        double z[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        st9(d.velgradold, N, v, z);
+        st9(d.dvr, N, v, z);
+        st6(d.sgt, N, v, z); st6(d.edotp, N, v, z); st6(d.ept, N, v, z); st6(d.disgradsym, N, v, z);
+        for (int s = 0; s < d.nsys; s++) {
+            d.gamdot[s * N + v] = 0.0;
+            d.crss[(2 * s) * N + v] = 0.0; d.crss[(2 * s + 1) * N + v] = 0.0;
+            d.trialtau[(2 * s) * N + v] = 0.0; d.trialtau[(2 * s + 1) * N + v] = 0.0;
+            for (int c = 0; c < 5; c++) d.sch[(s * 5 + c) * N + v] = 0.0;
+        }
+        if (ph.igas) {
+            st6(d.sg, N, v, z);
+            st9(d.ag, N, v, z);
+            for (int c = 0; c < 36; c++) d.sg66[c * N + v] = 0.0;
+            continue;
+        }
+        double aa[9], ag[9];
+        const double deg = EVP_PI / 180.0;
+        euler2(euler[3 * v] * deg, euler[3 * v + 1] * deg, euler[3 * v + 2] * deg, aa);
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) ag[3 * j + k] = aa[3 * k + j];
+        st9(d.ag, N, v, ag);
+        double c4[81], cg66[36];
+        rotate4(ag, ph.C, c4);
+        t4_to_b66(c4, cg66);
+        for (int c = 0; c < 36; c++) sums[c] += cg66[c] * d.wgt;
+        double sg6[6], s6[6];
+        for (int i = 0; i < 6; i++) {
+            double s = 0.0;
+            for (int j = 0; j < 6; j++) s += cg66[6 * i + j] * ip.u6t[j];
+            sg6[i] = s;
+        }
+        b6_to_s6(sg6, s6);
+        st6(d.sg, N, v, s6);
+        if (lu_inverse(cg66, 6) != 0) set_err(d.err, 1);
+        for (int c = 0; c < 36; c++) d.sg66[c * N + v] = cg66[c];
+        const double hps = hp[v];
+        for (int s = 0; s < ph.nsyst; s++) {
+            double c1 = ph.tau0f[s] + hps, c2 = ph.tau0b[s] + hps;
+            double db1 = ag[3] * ph.dbca[3 * s] + ag[4] * ph.dbca[3 * s + 1] + ag[5] * ph.dbca[3 * s + 2];
+            double cosalpha = fabs(db1);
+            c1 = c1 + ph.hpfac[s] * sqrt(cosalpha);
+            c2 = c2 + ph.hpfac[s] * sqrt(cosalpha);
+            d.crss[(2 * s) * N + v] = c1;
+            d.crss[(2 * s + 1) * N + v] = c2;
+            d.trialtau[(2 * s) * N + v] = c2;  // both columns start from the backward CRSS (IO_functions.f90:193-194)
+            d.trialtau[(2 * s + 1) * N + v] = c2;
+        }
+    }
+    reduce_store<36, 0>(sums, nullptr, d.partials, d.red + OFF_INIT, d.counters + CNT_INIT);
+}
+
+void launch_init(const Dev& d, const double* euler, const int* grain, const double* hp, const double* udot9, const double* u6t,
+                 cudaStream_t st) {
+    InitParams ip;
+    for (int c = 0; c < 9; c++) ip.udot[c] = udot9[c];
+    for (int c = 0; c < 6; c++) ip.u6t[c] = u6t[c];
+    k_init<<<d.grid, kBlock, 0, st>>>(d, euler, grain, hp, ip);
+}
+
+// ---------------------------------------------------------------- k_sgavg
+__global__ void __launch_bounds__(kBlock) k_sgavg(Dev d) {
+    const long long N = d.N;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        double w = d.wgtc[v];
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[c] += d.sg[c * N + v] * w;
+    }
+    reduce_store<6, 0>(s, nullptr, d.partials, d.red + OFF_SGAVG, d.counters + CNT_SGAVG);
+}
+void launch_sgavg(const Dev& d, cudaStream_t st) { k_sgavg<<<d.grid, kBlock, 0, st>>>(d); }
+
+// ---------------------------------------------------------------- k_prologue
+__global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __restrict__ c0g, const double* __restrict__ g0g,
+                                                       int do_schmid, int modal) {
+    __shared__ double c0[81], g0[81];
+    for (int i = threadIdx.x; i < 81; i += blockDim.x) {
+        c0[i] = c0g[i];
+        g0[i] = modal ? g0g[i] : 0.0;
+    }
+    __syncthreads();
+    const long long N = d.N;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const bool gas = d.gas[v];
+        if (do_schmid && !gas) {
+            const PhaseDev& ph = d.ph[d.phase[v]];
+            double Fe[9], ag[9], aa[9], ai[9];
+            ld9(d.Fe, N, v, Fe);
+            ld9(d.ag, N, v, ag);
+            mm3(Fe, ag, aa);
+            if (inv3(aa, ai) != 0) set_err(d.err, 1);
+            for (int s = 0; s < ph.nsyst; s++) {
+                double S[9], t[9], r[9], rs[9], b5[5];
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) S[3 * i + j] = ph.dbca[3 * s + i] * ph.dnca[3 * s + j];
+                mm3(aa, S, t);
+                mm3(t, ai, r);
+                sym33(r, rs);
+                t2_to_b5(rs, b5);
+                for (int c = 0; c < 5; c++) d.sch[(s * 5 + c) * N + v] = b5[c];
+            }
+        }
+        double F[9], detF = d.detF[v];
+        ld9(d.F, N, v, F);
+        double cm[81], cs[81], c66[36];
+        for (int ii = 0; ii < 3; ii++)
+            for (int jj = 0; jj < 3; jj++)
+                for (int kk = 0; kk < 3; kk++)
+                    for (int ll = 0; ll < 3; ll++) {
+                        double dum = 0.0;
+                        for (int m = 0; m < 3; m++)
+                            for (int n = 0; n < 3; n++) dum += c0[((ii * 3 + m) * 3 + kk) * 3 + n] * F[3 * jj + m] * F[3 * ll + n];
+                        cm[((ii * 3 + jj) * 3 + kk) * 3 + ll] = dum / detF;
+                    }
+        for (int ii = 0; ii < 3; ii++)
+            for (int jj = 0; jj < 3; jj++)
+                for (int kk = 0; kk < 3; kk++)
+                    for (int ll = 0; ll < 3; ll++)
+                        cs[((ii * 3 + jj) * 3 + kk) * 3 + ll] =
+                            0.25 * (cm[((ii * 3 + jj) * 3 + kk) * 3 + ll] + cm[((jj * 3 + ii) * 3 + kk) * 3 + ll] +
+                                    cm[((ii * 3 + jj) * 3 + ll) * 3 + kk] + cm[((jj * 3 + ii) * 3 + ll) * 3 + kk]);
+        t4_to_b66(cs, c66);
+        for (int c = 0; c < 36; c++) d.c066mod[c * N + v] = c66[c];
+        if (modal) {
+            double Fi[9], g66[36];
+            ld9(d.Finv, N, v, Fi);
+            for (int ii = 0; ii < 3; ii++)
+                for (int jj = 0; jj < 3; jj++)
+                    for (int kk = 0; kk < 3; kk++)
+                        for (int ll = 0; ll < 3; ll++) {
+                            double dum = 0.0;
+                            for (int m = 0; m < 3; m++)
+                                for (int n = 0; n < 3; n++) dum += g0[((ii * 3 + m) * 3 + kk) * 3 + n] * Fi[3 * m + jj] * Fi[3 * n + ll];
+                            cm[((ii * 3 + jj) * 3 + kk) * 3 + ll] = dum * detF;
+                        }
+            for (int ii = 0; ii < 3; ii++)
+                for (int jj = 0; jj < 3; jj++)
+                    for (int kk = 0; kk < 3; kk++)
+                        for (int ll = 0; ll < 3; ll++)
+                            cs[((ii * 3 + jj) * 3 + kk) * 3 + ll] =
+                                0.25 * (cm[((ii * 3 + jj) * 3 + kk) * 3 + ll] + cm[((jj * 3 + ii) * 3 + kk) * 3 + ll] +
+                                        cm[((ii * 3 + jj) * 3 + ll) * 3 + kk] + cm[((jj * 3 + ii) * 3 + ll) * 3 + kk]);
+            t4_to_b66(cs, g66);
+            for (int i = 0; i < 6; i++)
+                for (int j = 0; j < 6; j++) {
+                    double s = 0.0;
+                    for (int k = 0; k < 6; k++) s += c66[6 * i + k] * g66[6 * k + j];
+                    d.cG[(6 * i + j) * N + v] = s;
+                }
+        }
+    }
+}
+void launch_prologue(const Dev& d, const double* c0, const double* goperr0, int do_schmid, int modal, cudaStream_t st) {
+    k_prologue<<<d.grid, kBlock, 0, st>>>(d, c0, goperr0, do_schmid, modal);
+}
+
+// ---------------------------------------------------------------- k_gas_compl
+__global__ void __launch_bounds__(kBlock) k_gas_compl(Dev d, double tdot, double complgas, int modal) {
+    const long long N = d.N;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        if (!d.gas[v]) {
+            for (int c = 0; c < 36; c++) d.cgas[c * N + v] = 0.0;
+            continue;
+        }
+        double a[36];
+        for (int i = 0; i < 6; i++)
+            for (int j = 0; j < 6; j++) {
+                a[6 * i + j] = ((i == j) ? 1.0 : 0.0) + d.c066mod[(6 * i + j) * N + v] / tdot * complgas;
+                if (modal) a[6 * i + j] = a[6 * i + j] - d.cG[(6 * i + j) * N + v];
+            }
+        if (lu_inverse(a, 6) != 0) set_err(d.err, 1);
+        for (int c = 0; c < 36; c++) d.cgas[c * N + v] = a[c];
+    }
+}
+void launch_gas_compl(const Dev& d, double tdot, double complgas, int modal, cudaStream_t st) {
+    k_gas_compl<<<d.grid, kBlock, 0, st>>>(d, tdot, complgas, modal);
+}
+
+// ---------------------------------------------------------------- k_corr
+// velgrad += (dvelgradref + du) F^{-1}; averages; dL statistics; mixing.
+__global__ void __launch_bounds__(kBlock) k_corr(Dev d, CorrParams p) {
+    const long long N = d.N;
+    __shared__ double du[9];
+    if (threadIdx.x < 9) du[threadIdx.x] = __ldcg(&d.red[OFF_DU + threadIdx.x]);
+    __syncthreads();
+    double s[31];
+#pragma unroll
+    for (int c = 0; c < 31; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        double t[9], fi[9], u[9], vg[9], vo[9];
+        ld9(d.dvr, N, v, t);
+        ld9(d.Finv, N, v, fi);
+#pragma unroll
+        for (int c = 0; c < 9; c++) t[c] = t[c] + du[c];
+        mm3(t, fi, u);
+        ld9(d.velgrad, N, v, vg);
+        ld9(d.velgradold, N, v, vo);
+        const double w = d.wgtc[v];
+        const bool gas = d.gas[v];
+#pragma unroll
+        for (int c = 0; c < 9; c++) {
+            vg[c] = vg[c] + u[c];
+            s[c] += vg[c] * w;
+            if (gas) s[9 + c] += vg[c] * w;
+            else s[18 + c] += vg[c] * w;
+        }
+        if (!p.kinematic) {
+            double dl = 0.0;
+#pragma unroll
+            for (int c = 0; c < 9; c++) dl += (vg[c] - vo[c]) * (vg[c] - vo[c]);
+            dl = sqrt(dl);
+            double rel = dl / p.Lscale;
+            if (gas) { s[29] += (rel * rel) * w; s[30] += w; }
+            else { s[27] += (rel * rel) * w; s[28] += w; }
+        }
+#pragma unroll
+        for (int c = 0; c < 9; c++) vg[c] = p.do_mix ? p.mix * vg[c] + (1.0 - p.mix) * vo[c] : p.mix * vg[c];
+        st9(d.velgrad, N, v, vg);
+        st9(d.velgradold, N, v, vg);
+    }
+    reduce_store<31, 0>(s, nullptr, d.partials, d.red + OFF_CORR, d.counters + CNT_CORR);
+}
+void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st) { k_corr<<<d.grid, kBlock, 0, st>>>(d, p); }
+
+// ---------------------------------------------------------------- local constitutive solve
+// plastic_strain_rate (various_functions.f90:1367-1419) + elastic_strain_rate (1422-1436)
+template <int NS>
+__device__ __forceinline__ void constitutive(const PhaseDev& ph, const double* __restrict__ sch, long long N, long long v,
+                                             const double (&tt)[NS][2], const double (&sg)[6], double (&edotp)[6],
+                                             double (&dd)[15], double (&gamdot)[NS]) {
+#pragma unroll
+    for (int i = 0; i < 6; i++) edotp[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 15; i++) dd[i] = 0.0;
+#pragma unroll
+    for (int is = 0; is < NS; is++) {
+        if (is < ph.nsyst) {
+            double sc[5];
+#pragma unroll
+            for (int c = 0; c < 5; c++) sc[c] = sch[(is * 5 + c) * N + v];
+            double rss = sc[0] * sg[0] + sc[1] * sg[1] + sc[2] * sg[2] + sc[3] * sg[3] + sc[4] * sg[4];
+            const double tau = (rss - 0.0 < 0.0) ? tt[is][1] : tt[is][0];  // kin(is) == 0
+            rss = (rss - 0.0) / tau;
+            const double dum = ph.gamd0[is] * powabs(rss, ph.nrs[is] - 1.0, ph.int_exp);
+            const double rss1 = ph.nrs[is] * dum / tau;
+            const double rss2 = rss * dum;
+            gamdot[is] = rss2;
+            int q = 0;
+#pragma unroll
+            for (int jj = 0; jj < 5; jj++) {
+                edotp[jj] = edotp[jj] + sc[jj] * rss2;
+#pragma unroll
+                for (int ii = 0; ii <= jj; ii++) dd[q++] += sc[ii] * sc[jj] * rss1;
+            }
+        } else {
+            gamdot[is] = 0.0;
+        }
+    }
+}
+__device__ __forceinline__ double dd_at(const double (&dd)[15], int i, int j) {
+    if (i > 4 || j > 4) return 0.0;
+    int a = i < j ? i : j, b = i < j ? j : i;
+    return dd[b * (b + 1) / 2 + a];
+}
+
+// harden (various_functions.f90:1439-1491)
+template <int NS>
+__device__ __forceinline__ void harden(const PhaseDev& ph, const double* __restrict__ crss, long long N, long long v,
+                                       const double (&gamdot)[NS], double gamma0, double tdot, double (&tau)[NS][2], double& gamma1) {
+    double deltgam = 0.0;
+#pragma unroll
+    for (int is = 0; is < NS; is++)
+        if (is < ph.nsyst) deltgam = deltgam + fabs(gamdot[is]) * tdot;
+    gamma1 = gamma0 + deltgam;
+#pragma unroll
+    for (int is = 0; is < NS; is++) { tau[is][0] = 0.0; tau[is][1] = 0.0; }
+    int is = 0;
+    for (int mode = 0; mode < ph.nmodes; mode++) {
+        const double tau1 = ph.tau1[mode], thet0 = ph.thet0[mode], thet1 = ph.thet1[mode];
+        const double fact = fabs(thet0 / tau1);
+        const double exp0 = exp(-fact * gamma0), exp1 = exp(-fact * gamma1);
+        const double voce = deltgam * thet1 + tau1 * (exp0 - exp1) + thet1 * (gamma0 * exp0 - gamma1 * exp1);
+        for (int ism = 0; ism < ph.nsm[mode]; ism++, is++) {
+            double dtau = 0.;
+#pragma unroll
+            for (int js = 0; js < NS; js++)
+                if (js < ph.nsyst) dtau = dtau + ph.hard[is * kMaxSysDev + js] * fabs(gamdot[js]);
+#pragma unroll
+            for (int q = 0; q < NS; q++)
+                if (q == is) {
+                    tau[q][0] = crss[(2 * q) * N + v] + dtau * voce * tdot / deltgam;
+                    tau[q][1] = crss[(2 * q + 1) * N + v] + dtau * voce * tdot / deltgam;
+                }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- k_newton
+template <int NS>
+__global__ void __launch_bounds__(kNewtonBlock) k_newton(Dev d, NewtonParams p) {
+    const long long N = d.N;
+    double s[14];
+#pragma unroll
+    for (int c = 0; c < 14; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        double lam[6], sg[6], sgt[6], D[6];
+        {
+            double vg[9], vs[9], a[6];
+            ld9(d.velgrad, N, v, vg);
+            sym33(vg, vs);
+            t2_to_b6(vs, D);
+            ld6(d.sg, N, v, a);
+            s6_to_b6(a, lam);
+            ld6(d.sgt, N, v, a);
+            s6_to_b6(a, sgt);
+        }
+#pragma unroll
+        for (int i = 0; i < 6; i++) sg[i] = lam[i];
+        const double w = d.wgtc[v];
+        if (d.gas[v]) {
+            double t[6], res[6], out[6], s6v[6];
+#pragma unroll
+            for (int i = 0; i < 6; i++) t[i] = D[i] + sgt[i] / p.tdot * p.complgas;
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double a = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) a += d.c066mod[(6 * i + j) * N + v] * t[j];
+                res[i] = lam[i] + a;
+            }
+            if (p.modal) {
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 6; j++) a += d.cG[(6 * i + j) * N + v] * lam[j];
+                    res[i] -= a;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double a = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) a += d.cgas[(6 * i + j) * N + v] * res[j];
+                out[i] = a;
+            }
+            b6_to_s6(out, s6v);
+            st6(d.sg, N, v, s6v);
+            double z[6] = {0, 0, 0, 0, 0, 0};
+            st6(d.edotp, N, v, z);
+            for (int q = 0; q < d.nsys; q++) d.gamdot[q * N + v] = 0.0;
+#pragma unroll
+            for (int c = 0; c < 6; c++) s[8 + c] += s6v[c] * w;
+            continue;
+        }
+        const PhaseDev& ph = d.ph[d.phase[v]];
+        double tt[NS][2];
+        double taunrm = 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; q++) {
+            tt[q][0] = (q < d.nsys) ? d.trialtau[(2 * q) * N + v] : 0.0;
+            tt[q][1] = (q < d.nsys) ? d.trialtau[(2 * q + 1) * N + v] : 0.0;
+            taunrm += tt[q][0] * tt[q][0] + tt[q][1] * tt[q][1];
+        }
+        taunrm = sqrt(taunrm);
+        double edotth[6] = {0, 0, 0, 0, 0, 0};
+        if (p.thermo) {
+            double e9[9];
+            ld9(d.eth, N, v, e9);
+            t2_to_b6(e9, edotth);
+        }
+        double sgnorm = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; i++) sgnorm += sg[i] * sg[i];
+        sgnorm = sqrt(sgnorm);
+        const double tolt = fmax(p.error, p.erroral);
+        double errtau = 2.0 * tolt;
+        double edotp[6], dd[15], gamdot[NS], edot[6], res[6], sgold[6] = {0, 0, 0, 0, 0, 0};
+        double dsgnorm = 0.0, ddgnorm = 0.0;
+        const double gamma0 = d.gacumgr[v];
+        for (int itertau = 0; itertau < 10 && errtau > tolt;) {
+            itertau++;
+            int iterNR = 0;
+            double erral = 2.0 * p.erroral, resoldn = 1.0;
+            while (iterNR < 100 && erral > p.erroral) {
+                iterNR++;
+                int icut = 0;
+                double resn = 2.0 * resoldn;
+                while (resn > resoldn && icut < 10) {
+                    constitutive<NS>(ph, d.sch, N, v, tt, sg, edotp, dd, gamdot);
+                    double ds[6];
+#pragma unroll
+                    for (int i = 0; i < 6; i++) ds[i] = (sg[i] - sgt[i]) / p.tdot;
+#pragma unroll
+                    for (int i = 0; i < 6; i++) {
+                        double a = 0.0;
+#pragma unroll
+                        for (int j = 0; j < 6; j++) a += d.sg66[(6 * i + j) * N + v] * ds[j];
+                        edot[i] = edotp[i] + a;
+                        if (p.thermo) edot[i] = edot[i] + edotth[i];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 6; i++) {
+                        double a = 0.0;
+#pragma unroll
+                        for (int j = 0; j < 6; j++) a += d.c066mod[(6 * i + j) * N + v] * (edot[j] - D[j]);
+                        res[i] = sg[i] - lam[i] + a;
+                    }
+                    if (p.modal) {
+                        double r2[6];
+#pragma unroll
+                        for (int i = 0; i < 6; i++) {
+                            double a = 0.0;
+#pragma unroll
+                            for (int j = 0; j < 6; j++) a += d.cG[(6 * i + j) * N + v] * (sg[j] - lam[j]);
+                            r2[i] = a;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 6; i++) res[i] = res[i] - r2[i];
+                    }
+                    resn = 0.0;
+#pragma unroll
+                    for (int i = 0; i < 6; i++) resn += res[i] * res[i];
+                    resn = sqrt(resn);
+                    if (iterNR == 1) resoldn = resn;
+                    if (resn > resoldn) {
+#pragma unroll
+                        for (int i = 0; i < 6; i++) sg[i] = sgold[i] + (sg[i] - sgold[i]) * 0.5;
+                    }
+                    icut++;
+                }
+                resoldn = resn;
+#pragma unroll
+                for (int i = 0; i < 6; i++) sgold[i] = sg[i];
+                double J[36];
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    double crow[6];
+#pragma unroll
+                    for (int k = 0; k < 6; k++) crow[k] = d.c066mod[(6 * i + k) * N + v];
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        double a = 0.0;
+#pragma unroll
+                        for (int k = 0; k < 6; k++) a += crow[k] * (dd_at(dd, k, j) + d.sg66[(6 * k + j) * N + v] / p.tdot);
+                        J[6 * i + j] = ((i == j) ? 1.0 : 0.0) + a;
+                        if (p.modal) J[6 * i + j] -= d.cG[(6 * i + j) * N + v];
+                    }
+                }
+                if (solve6(J, res) != 0) set_err(d.err, 1);
+                double a = 0.0, b = 0.0, c = 0.0;
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    sg[i] = sg[i] - res[i];
+                    a += (sg[i] - sgold[i]) * (sg[i] - sgold[i]);
+                    b += (sg[i] - lam[i]) * (sg[i] - lam[i]);
+                    c += (edot[i] - D[i]) * (edot[i] - D[i]);
+                }
+                dsgnorm = b;
+                ddgnorm = c;
+                erral = sqrt(a) / sgnorm;
+            }
+            if (p.iuphard) {
+                double tn[NS][2], g1;
+                harden<NS>(ph, d.crss, N, v, gamdot, gamma0, p.tdot, tn, g1);
+                double e2 = 0.0;
+#pragma unroll
+                for (int q = 0; q < NS; q++) {
+                    e2 += (tt[q][0] - tn[q][0]) * (tt[q][0] - tn[q][0]) + (tt[q][1] - tn[q][1]) * (tt[q][1] - tn[q][1]);
+                    tt[q][0] = tn[q][0];
+                    tt[q][1] = tn[q][1];
+                }
+                errtau = sqrt(e2) / taunrm;
+            } else {
+                errtau = 0.0;
+            }
+        }
+        double s6v[6], e6v[6];
+        b6_to_s6(sg, s6v);
+        b6_to_s6(edotp, e6v);
+        st6(d.sg, N, v, s6v);
+        st6(d.edotp, N, v, e6v);
+#pragma unroll
+        for (int q = 0; q < NS; q++)
+            if (q < d.nsys) {
+                d.gamdot[q * N + v] = gamdot[q];
+                d.trialtau[(2 * q) * N + v] = tt[q][0];
+                d.trialtau[(2 * q + 1) * N + v] = tt[q][1];
+            }
+        if (!(dsgnorm == dsgnorm) || !(ddgnorm == ddgnorm)) set_err(d.err, 2);
+        s[0] += dsgnorm * w;
+        s[1] += ddgnorm * w;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            s[2 + c] += w * s6v[c];
+            s[8 + c] += s6v[c] * w;
+        }
+    }
+    reduce_store<14, 0>(s, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
+}
+void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
+    int grid = (int)((d.N + kNewtonBlock - 1) / kNewtonBlock);
+    if (grid > 148 * 16) grid = 148 * 16;
+    if (d.nsys <= 12) k_newton<12><<<grid, kNewtonBlock, 0, st>>>(d, p);
+    else k_newton<24><<<grid, kNewtonBlock, 0, st>>>(d, p);
+}
+
+// ---------------------------------------------------------------- k_upd1
+template <int NS>
+__global__ void __launch_bounds__(kBlock) k_upd1(Dev d, Upd1Params p) {
+    const long long N = d.N;
+    double s[39], mx[1] = {0.0};
+#pragma unroll
+    for (int c = 0; c < 39; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const bool gas = d.gas[v];
+        // accepted-step commit (LS-EVPFFT.f90:432-446)
+        double e6[6], a6[6], vg[9], vs[9];
+        ld6(d.edotp, N, v, e6);
+        ld6(d.ept, N, v, a6);
+#pragma unroll
+        for (int c = 0; c < 6; c++) a6[c] = a6[c] + e6[c] * p.tdot;
+        st6(d.ept, N, v, a6);
+        ld6(d.sg, N, v, a6);
+        st6(d.sgt, N, v, a6);
+        ld9(d.velgrad, N, v, vg);
+        sym33(vg, vs);
+        ld6(d.disgradsym, N, v, a6);
+        double vs6[6];
+        t2_to_s6(vs, vs6);
+#pragma unroll
+        for (int c = 0; c < 6; c++) a6[c] = a6[c] + vs6[c] * p.tdot;
+        st6(d.disgradsym, N, v, a6);
+        double e9[9];
+        s6_to_t2(e6, e9);
+        d.epvm[v] = d.epvm[v] + vm_strain(e9) * p.tdot;
+        const double evm = vm_strain(vs);
+        if (!gas) mx[0] = fmax(mx[0], evm);
+        if (!p.iupdate) continue;
+        if (!gas) {  // update_plastic_defgrad (various_functions.f90:1748-1827)
+            const PhaseDev& ph = d.ph[d.phase[v]];
+            double ag[9], Lp[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            ld9(d.ag, N, v, ag);
+            for (int is = 0; is < ph.nsyst; is++) {
+                double dn[3], db[3];
+                for (int i = 0; i < 3; i++) {
+                    dn[i] = ag[3 * i] * ph.dnca[3 * is] + ag[3 * i + 1] * ph.dnca[3 * is + 1] + ag[3 * i + 2] * ph.dnca[3 * is + 2];
+                    db[i] = ag[3 * i] * ph.dbca[3 * is] + ag[3 * i + 1] * ph.dbca[3 * is + 1] + ag[3 * i + 2] * ph.dbca[3 * is + 2];
+                }
+                const double gd = d.gamdot[is * N + v];
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) Lp[3 * i + j] = Lp[3 * i + j] + db[i] * dn[j] * gd;
+            }
+            double dl[9], ex[9], fp[9];
+            for (int c = 0; c < 9; c++) dl[c] = Lp[c] * p.tdot;
+            if (expm_adaptive(dl, ex) != 0) set_err(d.err, 1);
+            ld9(d.Fp, N, v, fp);
+            mm3(ex, fp, fp);
+            st9(d.Fp, N, v, fp);
+        }
+        // update_defgrad (various_functions.f90:2152-2282)
+        double dl[9], ex[9], F[9], Fi[9];
+        for (int c = 0; c < 9; c++) dl[c] = vg[c] * p.tdot;
+        if (expm_adaptive(dl, ex) != 0) set_err(d.err, 1);
+        ld9(d.F, N, v, F);
+        mm3(ex, F, F);
+        const double detF = det33(F);
+        if (inv3(F, Fi) != 0) set_err(d.err, 1);
+        st9(d.F, N, v, F);
+        st9(d.Finv, N, v, Fi);
+        st9(d.Finc, N, v, ex);
+        d.detF[v] = detF;
+        d.wgtc[v] = d.wgt * detF;
+#pragma unroll
+        for (int c = 0; c < 9; c++) {
+            s[c] += F[c] * d.wgt;
+            s[9 + c] += Fi[c] * d.wgt * detF;
+            if (gas) s[27 + c] += Fi[c] * d.wgt * detF;
+            else s[18 + c] += Fi[c] * d.wgt * detF;
+        }
+        if (gas) s[37] += d.wgt * detF;
+        else s[36] += d.wgt * detF;
+        s[38] += detF * d.wgt;
+    }
+    reduce_store<39, 1>(s, mx, d.partials, d.red + OFF_UPD1, d.counters + CNT_UPD1);
+}
+void launch_upd1(const Dev& d, const Upd1Params& p, cudaStream_t st) {
+    if (d.nsys <= 12) k_upd1<12><<<d.grid, kBlock, 0, st>>>(d, p);
+    else k_upd1<24><<<d.grid, kBlock, 0, st>>>(d, p);
+}
+
+// ---------------------------------------------------------------- k_upd2
+__global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
+    const long long N = d.N;
+    const double dav = __ldcg(&d.red[OFF_UPD1 + 38]);
+    double s[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const bool gas = d.gas[v];
+        const double w = d.wgtc[v] / dav;
+        d.wgtc[v] = w;
+        double Finc[9], Feinc[9];
+        ld9(d.Finc, N, v, Finc);
+        if (!gas) {
+            // update_elstic_defgrad (various_functions.f90:2285-2324), Fini = I
+            const PhaseDev& ph = d.ph[d.phase[v]];
+            double Fe[9], Feo[9], Fp[9], Fpi[9], F[9];
+            ld9(d.Fe, N, v, Fe);
+            if (inv3(Fe, Feo) != 0) set_err(d.err, 1);
+            ld9(d.Fp, N, v, Fp);
+            if (inv3(Fp, Fpi) != 0) set_err(d.err, 1);
+            ld9(d.F, N, v, F);
+            mm3(F, Fpi, Fe);
+            mm3(Fe, Feo, Feinc);
+            st9(d.Fe, N, v, Fe);
+            st9(d.Feinc, N, v, Feinc);
+            // update_el_stiff (various_functions.f90:2327-2402)
+            double ag[9], aa[9], c4[81], c66[36];
+            ld9(d.ag, N, v, ag);
+            mm3(Fe, ag, aa);
+            const double detFe = det33(Fe);
+            rotate4(aa, ph.C, c4);
+            for (int c = 0; c < 81; c++) c4[c] = c4[c] / detFe;
+            t4_to_b66(c4, c66);
+            if (lu_inverse(c66, 6) != 0) set_err(d.err, 1);
+            for (int c = 0; c < 36; c++) d.sg66[c * N + v] = c66[c];
+        } else {
+            ld9(d.Feinc, N, v, Feinc);
+        }
+        // update_tensor_config pass 1 (various_functions.f90:2425-2466)
+        const double detei = det33(Feinc);
+        double Fii[9];
+        if (inv3(Finc, Fii) != 0) set_err(d.err, 1);
+        if (!gas) {
+            double R[9], U[9], t[9], m[9], a6[6];
+            polar(Finc, R, U);
+            ld6(d.disgradsym, N, v, a6);
+            s6_to_t2(a6, m);
+            mm3(R, m, t);
+            mm3_bt(t, R, m);
+            t2_to_s6(m, a6);
+            st6(d.disgradsym, N, v, a6);
+            ld6(d.ept, N, v, a6);
+            s6_to_t2(a6, m);
+            mm3(R, m, t);
+            mm3_bt(t, R, m);
+            t2_to_s6(m, a6);
+            st6(d.ept, N, v, a6);
+            ld6(d.sgt, N, v, a6);
+            s6_to_t2(a6, m);
+            mm3(Feinc, m, t);
+            mm3_bt(t, Feinc, m);
+            for (int c = 0; c < 9; c++) m[c] = m[c] / detei;
+            t2_to_s6(m, a6);
+            st6(d.sgt, N, v, a6);
+        }
+        double vg[9];
+        ld9(d.velgrad, N, v, vg);
+        mm3(vg, Fii, vg);
+        st9(d.velgrad, N, v, vg);
+#pragma unroll
+        for (int c = 0; c < 9; c++) s[c] += vg[c] * w;
+    }
+    // reduce; the last block forms du2 = (<L>_prev - <L>) inv(<F^{-1}>_c)
+    __shared__ double sh[9][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int f = 0; f < 9; f++) {
+        double x = s[f];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[f][warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int f = 0; f < 9; f++) {
+            double x = lane < nw ? sh[f][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) d.partials[(size_t)blockIdx.x * 9 + f] = x;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(d.counters + CNT_UPD2, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double va[9], fc[9], di[9], dd[9], du[9];
+        for (int f = 0; f < 9; f++) {
+            double x = 0.0;
+            for (unsigned b = 0; b < gridDim.x; b++) x += __ldcg(&d.partials[(size_t)b * 9 + f]);
+            va[f] = x;
+            fc[f] = __ldcg(&d.red[OFF_UPD1 + 9 + f]) / dav;
+        }
+        if (inv3(fc, di) != 0) set_err(d.err, 1);
+        for (int f = 0; f < 9; f++) dd[f] = p.velgradavg[f] - va[f];
+        mm3(dd, di, du);
+        for (int f = 0; f < 9; f++) d.red[OFF_DU2 + f] = du[f];
+        d.counters[CNT_UPD2] = 0;
+    }
+}
+void launch_upd2(const Dev& d, const Upd2Params& p, cudaStream_t st) { k_upd2<<<d.grid, kBlock, 0, st>>>(d, p); }
+
+// ---------------------------------------------------------------- k_upd3
+template <int NS>
+__global__ void __launch_bounds__(kBlock) k_upd3(Dev d, Upd3Params p) {
+    const long long N = d.N;
+    __shared__ double du[9];
+    if (threadIdx.x < 9) du[threadIdx.x] = p.iupdate ? __ldcg(&d.red[OFF_DU2 + threadIdx.x]) : 0.0;
+    __syncthreads();
+    double s[30];
+#pragma unroll
+    for (int c = 0; c < 30; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const bool gas = d.gas[v];
+        if (p.iupdate) {
+            double fi[9], t[9], vg[9];
+            ld9(d.Finv, N, v, fi);
+            mm3(du, fi, t);
+            ld9(d.velgrad, N, v, vg);
+#pragma unroll
+            for (int c = 0; c < 9; c++) vg[c] = vg[c] + t[c];
+            st9(d.velgrad, N, v, vg);
+        }
+        if (gas) continue;
+        const PhaseDev& ph = d.ph[d.phase[v]];
+        double gd[NS];
+#pragma unroll
+        for (int q = 0; q < NS; q++) gd[q] = (q < d.nsys) ? d.gamdot[q * N + v] : 0.0;
+        if (p.iuphard) {  // update_hardening (various_functions.f90:1493-1523)
+            double tn[NS][2], g1;
+            harden<NS>(ph, d.crss, N, v, gd, d.gacumgr[v], p.tdot, tn, g1);
+#pragma unroll
+            for (int q = 0; q < NS; q++)
+                if (q < d.nsys) {
+                    d.crss[(2 * q) * N + v] = tn[q][0];
+                    d.crss[(2 * q + 1) * N + v] = tn[q][1];
+                    d.trialtau[(2 * q) * N + v] = tn[q][0];
+                    d.trialtau[(2 * q + 1) * N + v] = tn[q][1];
+                }
+            d.gacumgr[v] = g1;
+        }
+        const double w = d.wgtc[v];
+        double a[6];
+        ld6(d.ept, N, v, a);
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[c] += a[c] * w;
+        if (v == p.vlast) {
+            for (int c = 0; c < 6; c++) d.red[OFF_UPD3 + 36 + c] = a[c];
+        }
+        ld6(d.disgradsym, N, v, a);
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[6 + c] += a[c] * w;
+        if (v == p.vlast) {
+            for (int c = 0; c < 6; c++) d.red[OFF_UPD3 + 30 + c] = a[c];
+            d.red[OFF_UPD3 + 42] = w;
+        }
+        ld6(d.edotp, N, v, a);
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[12 + c] += a[c] * w;
+        ld6(d.sgt, N, v, a);
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[18 + c] += a[c] * w;
+        s[24] += d.gacumgr[v];
+        s[25] += 1.0;
+#pragma unroll
+        for (int q = 0; q < NS; q++)
+            if (q < ph.nsyst) {
+                const double gs = 0.5 * (d.crss[(2 * q) * N + v] + d.crss[(2 * q + 1) * N + v]);
+                s[26] += gs;
+                s[27] += 1.0;
+                s[28] += fabs(gd[q]);
+                s[29] += fabs(gd[q]) * gs;
+            }
+    }
+    reduce_store<30, 0>(s, nullptr, d.partials, d.red + OFF_UPD3, d.counters + CNT_UPD3);
+}
+void launch_upd3(const Dev& d, const Upd3Params& p, cudaStream_t st) {
+    if (d.nsys <= 12) k_upd3<12><<<d.grid, kBlock, 0, st>>>(d, p);
+    else k_upd3<24><<<d.grid, kBlock, 0, st>>>(d, p);
+}
+
+// ---------------------------------------------------------------- k_diag
+// sums: s2a swa s2s sws s2g swg | maxes: mxa mxs mxg vms vmg rms rmg sms smg ccs ccg cgg
+// min detF (all), and (min, last index) for solid and gas voxels.
+struct MinIdx {
+    double v;
+    long long i;
+};
+__device__ __forceinline__ MinIdx min_last(MinIdx a, MinIdx b) {
+    if (b.v < a.v) return b;
+    if (a.v < b.v) return a;
+    return (b.i > a.i) ? b : a;
+}
+__global__ void __launch_bounds__(kBlock) k_diag(Dev d, double Lfloor) {
+    const long long N = d.N;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    double m[13];
+#pragma unroll
+    for (int c = 0; c < 12; c++) m[c] = 0.0;
+    m[12] = -EVP_HUGE;  // max of -detF
+    MinIdx ms = {EVP_HUGE, -1}, mg = {EVP_HUGE, -1};
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const bool gas = d.gas[v];
+        double vg[9], vs[9], Fi[9];
+        ld9(d.velgrad, N, v, vg);
+        ld9(d.s_velgrad, N, v, vs);
+        double dl = 0.0, l0 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 9; c++) { dl += (vg[c] - vs[c]) * (vg[c] - vs[c]); l0 += vs[c] * vs[c]; }
+        dl = sqrt(dl);
+        l0 = sqrt(l0);
+        const double rel = dl / fmax(l0, Lfloor);
+        const double w = d.wgtc[v];
+        s[0] += (rel * rel) * w; s[1] += w; m[0] = fmax(m[0], rel);
+        const double detF = d.detF[v];
+        m[12] = fmax(m[12], -detF);
+        ld9(d.Finc, N, v, Fi);
+        double vi, ro, st, Ji;
+        stretch_rot(Fi, true, vi, ro, st, Ji);
+        double c66[36];
+        for (int c = 0; c < 36; c++) c66[c] = d.c066mod[c * N + v];
+        const double cc = cond1_est_6x6(c66);
+        if (gas) {
+            MinIdx t = {detF, v};
+            mg = min_last(mg, t);
+            s[4] += (rel * rel) * w; s[5] += w; m[2] = fmax(m[2], rel);
+            m[4] = fmax(m[4], vi); m[6] = fmax(m[6], ro); m[8] = fmax(m[8], st);
+            m[10] = fmax(m[10], cc);
+            for (int c = 0; c < 36; c++) c66[c] = d.cgas[c * N + v];
+            m[11] = fmax(m[11], cond1_est_6x6(c66));
+        } else {
+            MinIdx t = {detF, v};
+            ms = min_last(ms, t);
+            s[2] += (rel * rel) * w; s[3] += w; m[1] = fmax(m[1], rel);
+            m[3] = fmax(m[3], vi); m[5] = fmax(m[5], ro); m[7] = fmax(m[7], st);
+            m[9] = fmax(m[9], cc);
+        }
+    }
+    // (min, last index) pairs reduced first, by a fixed-order warp/block tree
+    __shared__ MinIdx shm[2][32];
+    __shared__ bool lastblk;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        MinIdx a = {__shfl_down_sync(0xffffffffu, ms.v, o), __shfl_down_sync(0xffffffffu, ms.i, o)};
+        MinIdx b = {__shfl_down_sync(0xffffffffu, mg.v, o), __shfl_down_sync(0xffffffffu, mg.i, o)};
+        ms = min_last(ms, a);
+        mg = min_last(mg, b);
+    }
+    if (lane == 0) { shm[0][warp] = ms; shm[1][warp] = mg; }
+    __syncthreads();
+    MinIdx* pm = reinterpret_cast<MinIdx*>(d.partials + (size_t)gridDim.x * 19);
+    if (threadIdx.x == 0) {
+        MinIdx a = shm[0][0], b = shm[1][0];
+        for (int q = 1; q < nw; q++) { a = min_last(a, shm[0][q]); b = min_last(b, shm[1][q]); }
+        pm[2 * blockIdx.x] = a;
+        pm[2 * blockIdx.x + 1] = b;
+    }
+    __syncthreads();
+    reduce_store<6, 13>(s, m, d.partials, d.red + OFF_DIAG, d.counters + CNT_DIAG);
+    // reduce_store reset the counter; use a second counter pass for the pairs
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) lastblk = (atomicAdd(d.counters + CNT_DIAG2, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (lastblk && threadIdx.x == 0) {
+        __threadfence();
+        MinIdx a = {EVP_HUGE, -1}, b = {EVP_HUGE, -1};
+        for (unsigned q = 0; q < gridDim.x; q++) {
+            MinIdx x = {__ldcg(&pm[2 * q].v), __ldcg(&pm[2 * q].i)};
+            MinIdx y = {__ldcg(&pm[2 * q + 1].v), __ldcg(&pm[2 * q + 1].i)};
+            a = min_last(a, x);
+            b = min_last(b, y);
+        }
+        d.red[OFF_DIAG + 19] = a.v;
+        d.red[OFF_DIAG + 20] = (double)a.i;
+        d.red[OFF_DIAG + 21] = b.v;
+        d.red[OFF_DIAG + 22] = (double)b.i;
+        d.counters[CNT_DIAG2] = 0;
+    }
+}
+void launch_diag(const Dev& d, double Lfloor, cudaStream_t st) { k_diag<<<d.grid, kBlock, 0, st>>>(d, Lfloor); }
+
+// ---------------------------------------------------------------- k_c0
+template <int NS>
+__global__ void __launch_bounds__(kBlock) k_c0(Dev d, double tdot, double tdotref) {
+    const long long N = d.N;
+    double s[117];
+#pragma unroll
+    for (int c = 0; c < 117; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        if (d.gas[v]) continue;
+        const PhaseDev& ph = d.ph[d.phase[v]];
+        double a6[6], sg[6];
+        ld6(d.sg, N, v, a6);
+        s6_to_b6(a6, sg);
+        double tt[NS][2], ep[6], dd[15], gd[NS];
+#pragma unroll
+        for (int q = 0; q < NS; q++) {
+            tt[q][0] = (q < d.nsys) ? d.trialtau[(2 * q) * N + v] : 1.0;
+            tt[q][1] = (q < d.nsys) ? d.trialtau[(2 * q + 1) * N + v] : 1.0;
+        }
+        constitutive<NS>(ph, d.sch, N, v, tt, sg, ep, dd, gd);
+        double tr[36];
+        for (int i = 0; i < 6; i++)
+            for (int j = 0; j < 6; j++) tr[6 * i + j] = d.sg66[(6 * i + j) * N + v] / tdot * tdot / tdotref + dd_at(dd, i, j);
+        if (lu_inverse(tr, 6) != 0) set_err(d.err, 1);
+        double dsg[81], dpg[81], dp6[36], Fi[9];
+        b66_to_t4(tr, dsg);
+        ld9(d.Finv, N, v, Fi);
+        const double detF = d.detF[v], w = d.wgtc[v];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                for (int k = 0; k < 3; k++)
+                    for (int l = 0; l < 3; l++) {
+                        double x = 0.0;
+                        for (int m = 0; m < 3; m++)
+                            for (int n = 0; n < 3; n++) x = x + dsg[((i * 3 + m) * 3 + k) * 3 + n] * Fi[3 * j + m] * Fi[3 * l + n] * detF;
+                        dpg[((i * 3 + j) * 3 + k) * 3 + l] = x;
+                    }
+        t4_to_b66(dpg, dp6);
+        for (int c = 0; c < 81; c++) s[c] += dsg[c] * w;
+        for (int c = 0; c < 36; c++) s[81 + c] += dp6[c] * d.wgt;
+    }
+    reduce_store<117, 0>(s, nullptr, d.partials, d.red + OFF_C0, d.counters + CNT_C0);
+}
+void launch_c0(const Dev& d, double tdot, double tdotref, cudaStream_t st) {
+    if (d.nsys <= 12) k_c0<12><<<d.grid, kBlock, 0, st>>>(d, tdot, tdotref);
+    else k_c0<24><<<d.grid, kBlock, 0, st>>>(d, tdot, tdotref);
+}
+
+// ---------------------------------------------------------------- k_kinematic
+__global__ void __launch_bounds__(kBlock) k_kinematic(Dev d, double tdot_step) {
+    const long long N = d.N;
+    double m[4] = {0.0, 0.0, 0.0, -EVP_HUGE};
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        double L[9], Fi[9];
+        ld9(d.velgrad, N, v, L);
+        for (int c = 0; c < 9; c++) L[c] = L[c] * tdot_step;
+        if (expm_adaptive(L, Fi) != 0) set_err(d.err, 1);
+        double vi, ro, st, Ji;
+        stretch_rot(Fi, false, vi, ro, st, Ji);
+        m[0] = fmax(m[0], vi);
+        m[1] = fmax(m[1], ro);
+        m[2] = fmax(m[2], st);
+        m[3] = fmax(m[3], -(d.detF[v] * Ji));
+    }
+    reduce_store<0, 4>(nullptr, m, d.partials, d.red + OFF_KIN, d.counters + CNT_KIN);
+}
+void launch_kinematic(const Dev& d, double tdot_step, cudaStream_t st) { k_kinematic<<<d.grid, kBlock, 0, st>>>(d, tdot_step); }
+
+// ---------------------------------------------------------------- k_cell2node
+__global__ void __launch_bounds__(kBlock) k_cell2node(Dev d, double tdot, int ideriv) {
+    const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+    const long long nn1 = n1 + 1, nn2 = n2 + 1;
+    const long long nnode = nn1 * nn2 * d.n3node;
+    __shared__ double va[9];
+    if (threadIdx.x < 9) va[threadIdx.x] = __ldcg(&d.red[OFF_DC + 2 * threadIdx.x]) * d.wgt;
+    __syncthreads();
+    const long long N = d.N;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nnode; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % nn1) + 1, j = (int)((q / nn1) % nn2) + 1, k = (int)(q / (nn1 * nn2)) + 1;
+        double dn[3];
+        if (ideriv != 2) {
+            int k1 = k - 1, k2 = k, j1 = j - 1, j2 = j, i1 = i - 1, i2 = i;
+            if (k1 == 0) k1 = n3;
+            if (k2 == n3 + 1) k2 = 1;
+            if (j1 == 0) j1 = n2;
+            if (j2 == n2 + 1) j2 = 1;
+            if (i1 == 0) i1 = n1;
+            if (i2 == n1 + 1) i2 = 1;
+            auto c = [&](int a, int b, int e, int l) {
+                return d.dv3[l * N + (a - 1) + (long long)n1 * ((b - 1) + (long long)n2 * (e - 1))];
+            };
+            for (int l = 0; l < 3; l++)
+                dn[l] = (c(i2, j2, k2, l) + c(i1, j2, k2, l) + c(i2, j1, k2, l) + c(i2, j2, k1, l) + c(i1, j1, k2, l) +
+                         c(i1, j2, k1, l) + c(i2, j1, k1, l) + c(i1, j1, k1, l)) * 0.125;
+        } else {
+            long long vv = ((i - 1) % n1) + (long long)n1 * (((j - 1) % n2) + (long long)n2 * ((k - 1) % n3));
+            for (int l = 0; l < 3; l++) dn[l] = d.dv3[l * N + vv];
+        }
+        const double x[3] = {(double)i - 0.5, (double)j - 0.5, (d.n3node == 1) ? 0.0 : (double)k - 0.5};
+        for (int l = 0; l < 3; l++) {
+            const double sv = va[3 * l] * x[0] + va[3 * l + 1] * x[1] + va[3 * l + 2] * x[2];
+            d.xnode[3 * q + l] = d.xnode[3 * q + l] + (sv + dn[l]) * tdot;
+        }
+    }
+}
+void launch_cell2node(const Dev& d, double tdot, int ideriv, cudaStream_t st) {
+    k_cell2node<<<d.grid, kBlock, 0, st>>>(d, tdot, ideriv);
+}
+
+// ---------------------------------------------------------------- k_goperr0
+// Goperr0 = (1/N) sum_k Re Gamma(k) over the full grid (igamma = 0).
+__device__ __forceinline__ void spatial_freq(int kx, int ky, int kz, int n1, int n2, int n3, double* xi) {
+    const double twopi = 2.0 * EVP_PI;
+    xi[0] = (kx + 1 <= n1 / 2) ? twopi * (double)kx / (double)n1 : twopi * (double)(kx - n1) / (double)n1;
+    xi[1] = (ky + 1 <= n2 / 2) ? twopi * (double)ky / (double)n2 : twopi * (double)(ky - n2) / (double)n2;
+    if (n3 == 1) xi[2] = 0.0;
+    else xi[2] = (kz + 1 <= n3 / 2) ? twopi * (double)kz / (double)n3 : twopi * (double)(kz - n3) / (double)n3;
+}
+__global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restrict__ c0g, const double* __restrict__ s0g) {
+    __shared__ double c0[81], s0[81];
+    for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = c0g[i]; s0[i] = s0g[i]; }
+    __syncthreads();
+    const long long N = d.N;
+    const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+    double s[81];
+#pragma unroll
+    for (int c = 0; c < 81; c++) s[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const int kx = (int)(v % n1), ky = (int)((v / n1) % n2), kz = (int)(v / ((long long)n1 * n2));
+        const bool nyq = (n1 % 2 == 0 && kx == n1 / 2) || (n2 % 2 == 0 && ky == n2 / 2) || (n3 % 2 == 0 && kz == n3 / 2 && n3 > 1);
+        if (nyq) {
+            for (int c = 0; c < 81; c++) s[c] += -s0[c];
+            continue;
+        }
+        if (v == 0) continue;
+        double xi[3], A[9], a[9];
+        spatial_freq(kx, ky, kz, n1, n2, n3, xi);
+        for (int i = 0; i < 3; i++)
+            for (int k = 0; k < 3; k++) {
+                double x = 0.0;
+                for (int j = 0; j < 3; j++)
+                    for (int l = 0; l < 3; l++) x += c0[((i * 3 + j) * 3 + k) * 3 + l] * (xi[j] * xi[l]);
+                A[3 * i + k] = x;
+            }
+        if (inv3(A, a) != 0) set_err(d.err, 1);
+        for (int p = 0; p < 3; p++)
+            for (int q = 0; q < 3; q++)
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) s[((p * 3 + q) * 3 + i) * 3 + j] += -a[3 * p + i] * (xi[q] * xi[j]);
+    }
+    reduce_store<81, 0>(s, nullptr, d.partials, d.red + OFF_G0, d.counters + CNT_G0);
+}
+void launch_goperr0(const Dev& d, const double* c0, const double* s0, cudaStream_t st) {
+    k_goperr0<<<d.grid, kBlock, 0, st>>>(d, c0, s0);
+}
+
+}  // namespace evp

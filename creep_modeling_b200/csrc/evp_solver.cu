@@ -1,0 +1,1159 @@
+// evp_solver.cu -- host orchestration of one LS-EVPFFT solve on a B200 and the C ABI.
+//
+// The macrostep / equilibrium-iteration control flow of lsevpfft/src/LS-EVPFFT.f90
+// runs here on the host; every per-voxel and per-frequency loop runs on the
+// device (evp_kernels.cu, evp_fft.cu).  Per equilibrium iteration the host
+// launches seven kernels and reads back one small block of sums; the serial
+// 6x6 / 3x3 tails of the reference (state_6x6_evpsc, calc_velgradavg_corr,
+// calc_c0, convergence and time-step control) run on those sums in FP64.
+#include "../../include/evp.h"
+#include "evp_deck.h"
+#include "evp_dev.cuh"
+#include "evp_math.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <vector>
+#include <sys/stat.h>
+
+namespace evp {
+
+static thread_local std::string g_last_error;
+
+struct SolveError : std::runtime_error {
+    int code;
+    SolveError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                              \
+    do {                                                                                                   \
+        cudaError_t e_ = (x);                                                                              \
+        if (e_ != cudaSuccess) throw SolveError(std::string("CUDA error: ") + cudaGetErrorString(e_), -6); \
+    } while (0)
+
+static void mkdir_p(const std::string& dir) {
+    std::string cur;
+    for (size_t i = 0; i <= dir.size(); i++) {
+        if (i == dir.size() || dir[i] == '/')
+            if (!cur.empty()) ::mkdir(cur.c_str(), 0755);
+        if (i < dir.size()) cur += dir[i];
+    }
+}
+static std::string g0(double x) {
+    char b[40];
+    std::snprintf(b, sizeof(b), "%.17g", x);
+    return b;
+}
+// Fortran E18.8E3 (write_vtk_cell)
+static void put_e18(std::string& o, double x) {
+    if (std::fabs(x) < EVP_TINY) x = 0.0;  // clamp_subnormal (IO_functions.f90:938-943)
+    char m[40], b[40];
+    if (x == 0.0) {
+        std::snprintf(b, sizeof(b), "%18s", "0.00000000E+000");
+        o += b;
+        return;
+    }
+    std::snprintf(m, sizeof(m), "%.7e", std::fabs(x));
+    int e10 = std::atoi(m + 10) + 1;
+    char dg[9];
+    dg[0] = m[0];
+    std::memcpy(dg + 1, m + 2, 7);
+    dg[8] = 0;
+    char body[40];
+    std::snprintf(body, sizeof(body), "%s0.%sE%c%03d", x < 0 ? "-" : "", dg, e10 < 0 ? '-' : '+', e10 < 0 ? -e10 : e10);
+    std::snprintf(b, sizeof(b), "%18s", body);
+    o += b;
+}
+
+struct Diag {
+    double detF_min = 0, detF_min_sol = 0, detF_min_gas = 0, detF_min_prev = 0, detF_min_sol_prev = 0, detF_min_gas_prev = 0;
+    double detF_min_sol_rel = 0, detF_min_gas_rel = 0;
+    double volinc_sol = 0, volinc_gas = 0, volinc_sol_prev = 0, volinc_gas_prev = 0, volinc_sol_rel = 0, volinc_gas_rel = 0;
+    double stretch_sol = 0, stretch_gas = 0, stretch_sol_prev = 0, stretch_gas_prev = 0, stretch_sol_rel = 0, stretch_gas_rel = 0;
+    double rot_sol = 0, rot_gas = 0;
+    double dl_rms_sol = 0, dl_rms_gas = 0, dl_rms = 0, dl_max_sol = 0, dl_max_gas = 0, dl_max = 0;
+    double dvelgradavg_mag = 0, erre = 0, errs = 0, errsbc = 0, tdotref = 0, devm_inc_max = 0, s33_target = 0, s33 = 0, s33_sol = 0;
+    double cond_sol = 0, cond_gas = 0, cond_cgas = 0;
+    int imin_sol[3] = {0, 0, 0}, imin_gas[3] = {0, 0, 0};
+};
+static double safe_rel(double x, double xp) { return (xp <= EVP_TINY || xp >= EVP_HUGE * 0.5) ? 0.0 : std::fabs(x - xp) / xp; }
+
+class Solver {
+public:
+    Deck dk;
+    Dev d{};
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    FftPlan1D pl1{}, pl2{}, pl3{};
+    std::vector<void*> allocs;
+    double* h_red = nullptr;  // pinned copy of the result buffer
+    int* h_err = nullptr;
+    double *d_c0 = nullptr, *d_s0 = nullptr, *d_g0 = nullptr;
+    // macro state (micro_type, types.f90:55-94)
+    double c066[36] = {}, s066[36] = {}, c0[81] = {}, s0[81] = {}, de_ds[81] = {}, goperr0[81] = {};
+    double wphsol = 0, wphgas = 0, wphcsol = 0, wphcgas = 0;
+    double defgradavg[9], dinvc[9], dinvcs[9], dinvcg[9];
+    double dvelgradavg[9] = {}, velgradavg[9] = {}, velgradavgsol[9] = {}, velgradavggas[9] = {};
+    double sgavg[9] = {}, sgavgsol[9] = {}, sgsolavg[9] = {};
+    double svmavg = 0, dvmavg = 0, edotvmmx = 0, evmavg = 0, evmpavg = 0, dvmpavg = 0, lvmavg = 0;
+    double epavg[9] = {}, eavg[9] = {}, eelavg[9] = {}, edotpavg[9] = {};
+    Diag dg;
+    // driver state (global.f90:19-27, LS-EVPFFT.f90:15-82)
+    int ipr = 0, imacroloop = 1, imicro = 0, iter = 0, nconverged = 0, total_macrosteps = 0;
+    double erre = 0, errs = 0, errsbc = 0, mix = 1.0, sim_time = 0, wall_time = 0, tdot_plan = 0, proc_time_target = 0,
+           proc_time_done = 0;
+    bool kinematic = false, do_mix = true, modal = false, write_files = false, verbose = false, finished = false;
+    long long vlast = -1;
+    long long total_iters = 0;
+    int macrosteps_done = 0;
+    double gpu_ms = 0.0;
+    std::time_t start = 0;
+    std::string outdir;
+    double last_results[53] = {}, last_diag[44] = {};
+    std::vector<double> snap_dsim, snap_scau;
+    bool has_thermo = false;
+
+    ProcessData& P() { return dk.process[ipr - 1]; }
+
+    template <class T>
+    T* dalloc(size_t n) {
+        void* p = nullptr;
+        if (n == 0) return nullptr;
+        CK(cudaMalloc(&p, n * sizeof(T)));
+        allocs.push_back(p);
+        return (T*)p;
+    }
+    ~Solver() {
+        for (void* p : allocs) cudaFree(p);
+        if (h_red) cudaFreeHost(h_red);
+        if (h_err) cudaFreeHost(h_err);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    void sync() { CK(cudaStreamSynchronize(st)); }
+    void fetch_red() {
+        CK(cudaMemcpyAsync(h_red, d.red, RED_OUT_SIZE * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(h_err, d.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        sync();
+        if (*h_err & 1) throw SolveError("singular matrix in a voxel operator (lu_inverse / lu_eqsystem)", -3);
+        if (*h_err & 2) throw SolveError("non-finite stress in the local Newton solve", -4);
+    }
+
+    // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
+    void open(const std::string& fft_in, const std::string& out, int mix_flag, int modal_flag, int flags) {
+        write_files = (flags & EVP_WRITE_FILES) != 0;
+        verbose = (flags & EVP_VERBOSE) != 0;
+        outdir = out.empty() ? std::string("evpfft_outputs/") : out;
+        if (write_files) {
+            mkdir_p(outdir);
+            // old *.vtk / *.out are removed at start (LS-EVPFFT.f90:145-146)
+            std::string cmd = "find \"" + outdir + "\" -maxdepth 1 -type f \\( -name '*.vtk' -o -name '*.out' \\) -delete 2>/dev/null";
+            if (std::system(cmd.c_str()) != 0) {}
+        }
+        try {
+            dk = parse_deck(fft_in);
+        } catch (DeckError& e) {
+            throw SolveError(e.what(), e.code);
+        }
+        for (auto& p : dk.process)
+            if (p.igamma != 0) throw SolveError("IGAMMA = 1 or 2 (discrete Green operators) is not supported by this build", -2);
+        int dev_count = 0;
+        if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) throw SolveError("no CUDA device available", -6);
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        static bool configured = false;
+        if (!configured) { fft_configure(); configured = true; }
+        allocate();
+        upload_and_init();
+        modal = (modal_flag != 0);
+        do_mix = (mix_flag != 0);
+        start = std::time(nullptr);
+        const ProcessData& p1 = dk.process[0];
+        dvmavg = vm_strain(p1.dsim);
+        lvmavg = dvmavg;
+        if (write_files) write_vtk(0);
+        // start-up tangent (LS-EVPFFT.f90:156-173)
+        for (int c = 0; c < 36; c++) c066[c] = h_red[OFF_INIT + c] / wphcsol * p1.tdot;
+        for (int c = 0; c < 36; c++) s066[c] = c066[c];
+        if (lu_inverse(s066, 6) != 0) throw SolveError("Singular matrix in lu_inverse (start-up c066)", -3);
+        b66_to_t4(c066, c0);
+        b66_to_t4(s066, s0);
+        std::memcpy(de_ds, s0, sizeof(de_ds));
+        upload_c0();
+        if (write_files) write_headers();
+        for (auto& p : dk.process) total_macrosteps += p.nsteps;
+        imacroloop = 1;
+        ipr = 0;
+        imicro = 0;
+    }
+
+    void allocate() {
+        const long long N = dk.nvox();
+        d.N = N;
+        d.n1 = dk.n1; d.n2 = dk.n2; d.n3 = dk.n3;
+        d.n1h = dk.n1 / 2 + 1;
+        d.n3node = (dk.n3 == 1) ? 1 : dk.n3 + 1;
+        d.wgt = dk.wgt;
+        int ns = 1;
+        for (auto& ph : dk.phase) ns = std::max(ns, ph.nsyst);
+        d.nsys = ns;
+        long long g = (N + 255) / 256;
+        d.grid = (int)std::min<long long>(g, 148LL * 8);
+        d.sg = dalloc<double>(6 * N); d.sgt = dalloc<double>(6 * N); d.edotp = dalloc<double>(6 * N);
+        d.ept = dalloc<double>(6 * N); d.disgradsym = dalloc<double>(6 * N);
+        d.velgrad = dalloc<double>(9 * N); d.velgradold = dalloc<double>(9 * N); d.dvr = dalloc<double>(9 * N);
+        d.F = dalloc<double>(9 * N); d.Finv = dalloc<double>(9 * N); d.Fe = dalloc<double>(9 * N); d.Fp = dalloc<double>(9 * N);
+        d.Finc = dalloc<double>(9 * N); d.Feinc = dalloc<double>(9 * N); d.ag = dalloc<double>(9 * N);
+        d.detF = dalloc<double>(N); d.wgtc = dalloc<double>(N); d.epvm = dalloc<double>(N); d.gacumgr = dalloc<double>(N);
+        d.sg66 = dalloc<double>(36 * N); d.c066mod = dalloc<double>(36 * N);
+        d.cG = dalloc<double>(36 * N);
+        d.cgas = dk.has_gas ? dalloc<double>(36 * N) : nullptr;
+        d.sch = dalloc<double>(5 * (size_t)ns * N);
+        d.crss = dalloc<double>(2 * (size_t)ns * N); d.trialtau = dalloc<double>(2 * (size_t)ns * N);
+        d.gamdot = dalloc<double>((size_t)ns * N);
+        d.eth = dk.eth.empty() ? nullptr : dalloc<double>(9 * N);
+        d.gas = dalloc<uint8_t>(N); d.phase = dalloc<uint8_t>(N);
+        d.s_velgrad = dalloc<double>(9 * N); d.s_velgradold = dalloc<double>(9 * N); d.s_sg = dalloc<double>(6 * N);
+        d.s_edotp = dalloc<double>(6 * N); d.s_gamdot = dalloc<double>((size_t)ns * N); d.s_trialtau = dalloc<double>(2 * (size_t)ns * N);
+        d.spec = dalloc<double2>(9 * (size_t)d.n1h * dk.n2 * dk.n3);
+        d.tw1 = dalloc<double2>(dk.n1); d.tw2 = dalloc<double2>(dk.n2); d.tw3 = dalloc<double2>(dk.n3);
+        d.dv3 = dalloc<double>(3 * N);
+        d.xnode = dalloc<double>(3 * (size_t)(dk.n1 + 1) * (dk.n2 + 1) * d.n3node);
+        d.partials = dalloc<double>(200 * 2048);
+        d.red = dalloc<double>(RED_OUT_SIZE);
+        d.counters = dalloc<unsigned int>(CNT_N);
+        d.err = dalloc<int>(1);
+        CK(cudaMemsetAsync(d.counters, 0, CNT_N * sizeof(unsigned int), st));
+        CK(cudaMemsetAsync(d.err, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(d.red, 0, RED_OUT_SIZE * sizeof(double), st));
+        CK(cudaMemsetAsync(d.cG, 0, 36 * N * sizeof(double), st));
+        d_c0 = dalloc<double>(81); d_s0 = dalloc<double>(81); d_g0 = dalloc<double>(81);
+        CK(cudaMemsetAsync(d_g0, 0, 81 * sizeof(double), st));
+        CK(cudaMallocHost(&h_red, RED_OUT_SIZE * sizeof(double)));
+        CK(cudaMallocHost(&h_err, sizeof(int)));
+        pl1 = make_plan(dk.n1); pl2 = make_plan(dk.n2); pl3 = make_plan(dk.n3);
+        auto twiddles = [&](int n, double2* dst) {
+            std::vector<double2> t(n);
+            for (int e = 0; e < n; e++) {
+                long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)n;
+                t[e] = make_double2((double)cosl(ang), (double)sinl(ang));
+            }
+            CK(cudaMemcpyAsync(dst, t.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+            sync();
+        };
+        twiddles(dk.n1, d.tw1); twiddles(dk.n2, d.tw2); twiddles(dk.n3, d.tw3);
+        // phases
+        std::vector<PhaseDev> ph(dk.nph);
+        for (int p = 0; p < dk.nph; p++) {
+            const PhaseData& s = dk.phase[p];
+            PhaseDev& t = ph[p];
+            std::memset(&t, 0, sizeof(t));
+            t.nsyst = s.nsyst; t.nmodes = s.nmodes; t.igas = s.igas ? 1 : 0;
+            t.int_exp = 1;
+            for (int m = 0; m < 3; m++) t.nsm[m] = s.nsm[m];
+            int islast = 0;
+            for (int m = 0; m < s.nmodes; m++) {
+                islast += s.nsm[m];
+                t.tau1[m] = s.tau[islast - 1][2];
+                t.thet0[m] = s.thet[islast - 1][0];
+                t.thet1[m] = s.thet[islast - 1][1];
+            }
+            for (int i = 0; i < kMaxSys; i++) {
+                t.nrs[i] = s.nrs[i]; t.gamd0[i] = s.gamd0[i]; t.hpfac[i] = s.hpfac[i];
+                t.tau0f[i] = s.tau[i][0]; t.tau0b[i] = s.tau[i][1];
+                for (int j = 0; j < kMaxSys; j++) t.hard[i * kMaxSysDev + j] = s.hard[i][j];
+                for (int c = 0; c < 3; c++) { t.dnca[3 * i + c] = s.dnca[i][c]; t.dbca[3 * i + c] = s.dbca[i][c]; }
+                if (i < s.nsyst) {
+                    double e = s.nrs[i] - 1.0;
+                    if (!(e >= 0.0 && e <= 64.0 && e == std::floor(e))) t.int_exp = 0;
+                }
+            }
+            for (int c = 0; c < 81; c++) t.C[c] = s.C[c];
+        }
+        PhaseDev* dph = dalloc<PhaseDev>(dk.nph);
+        CK(cudaMemcpyAsync(dph, ph.data(), dk.nph * sizeof(PhaseDev), cudaMemcpyHostToDevice, st));
+        d.ph = dph;
+        d.nph = dk.nph;
+    }
+
+    void upload_and_init() {
+        const long long N = d.N;
+        std::vector<uint8_t> gas(N), phs(N);
+        wphsol = 0.0; wphgas = 0.0;
+        for (long long v = 0; v < N; v++) {
+            phs[v] = (uint8_t)(dk.phase_id[v] - 1);
+            gas[v] = dk.phase[dk.phase_id[v] - 1].igas ? 1 : 0;
+            if (gas[v]) wphgas += dk.wgt;
+            if (!gas[v]) { wphsol += dk.wgt; vlast = v; }
+        }
+        wphcsol = wphsol;
+        wphcgas = wphgas;
+        for (int c = 0; c < 9; c++) {
+            defgradavg[c] = dinvc[c] = dinvcs[c] = dinvcg[c] = (c % 4 == 0) ? 1.0 : 0.0;
+        }
+        CK(cudaMemcpyAsync(d.gas, gas.data(), N, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.phase, phs.data(), N, cudaMemcpyHostToDevice, st));
+        if (d.eth) CK(cudaMemcpyAsync(d.eth, dk.eth.data(), 9 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+        for (auto& p : dk.process) has_thermo = has_thermo || p.ithermo == 1;
+        double* d_eul = dalloc<double>(3 * N);
+        int* d_gr = dalloc<int>(N);
+        double* d_hp = dalloc<double>(N);
+        CK(cudaMemcpyAsync(d_eul, dk.euler.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_gr, dk.grain.data(), N * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_hp, dk.hp_shift.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+        // xnode start values (types.f90:273-287)
+        {
+            const int n1 = dk.n1, n2 = dk.n2, nn3 = d.n3node;
+            std::vector<double> xn(3 * (size_t)(n1 + 1) * (n2 + 1) * nn3);
+            for (int k = 0; k < nn3; k++)
+                for (int j = 0; j < n2 + 1; j++)
+                    for (int i = 0; i < n1 + 1; i++) {
+                        size_t p = 3 * (i + (size_t)(n1 + 1) * (j + (size_t)(n2 + 1) * k));
+                        xn[p] = (double)(i + 1) - 0.5;
+                        xn[p + 1] = (double)(j + 1) - 0.5;
+                        xn[p + 2] = (nn3 == 1) ? 0.0 : (double)(k + 1) - 0.5;
+                    }
+            CK(cudaMemcpyAsync(d.xnode, xn.data(), xn.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        const ProcessData& p1 = dk.process[0];
+        double u6[6], u6t[6];
+        t2_to_b6(p1.udot, u6);
+        for (int c = 0; c < 6; c++) u6t[c] = u6[c] * p1.tdot;
+        launch_init(d, d_eul, d_gr, d_hp, p1.udot, u6t, st);
+        CK(cudaGetLastError());
+        fetch_red();
+        // release the start-up staging buffers
+        for (void* p : {(void*)d_eul, (void*)d_gr, (void*)d_hp}) {
+            cudaFree(p);
+            allocs.erase(std::find(allocs.begin(), allocs.end(), p));
+        }
+    }
+
+    void upload_c0() {
+        CK(cudaMemcpyAsync(d_c0, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_s0, s0, sizeof(s0), cudaMemcpyHostToDevice, st));
+    }
+
+    // ------------------------------------------------------------ snapshots (various_functions.f90:2839-2895)
+    void snapshot(bool take) {
+        const long long N = d.N;
+        const size_t ns = d.nsys;
+        auto cp = [&](double* dst, double* src, size_t n) {
+            CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        };
+        ProcessData& p = P();
+        if (take) {
+            snap_dsim.assign(p.dsim, p.dsim + 9);
+            snap_scau.assign(p.scauchy, p.scauchy + 9);
+            cp(d.s_velgrad, d.velgrad, 9 * N); cp(d.s_velgradold, d.velgradold, 9 * N); cp(d.s_sg, d.sg, 6 * N);
+            cp(d.s_edotp, d.edotp, 6 * N); cp(d.s_gamdot, d.gamdot, ns * N); cp(d.s_trialtau, d.trialtau, 2 * ns * N);
+        } else {
+            std::memcpy(p.dsim, snap_dsim.data(), 9 * sizeof(double));
+            std::memcpy(p.scauchy, snap_scau.data(), 9 * sizeof(double));
+            cp(d.velgrad, d.s_velgrad, 9 * N); cp(d.velgradold, d.s_velgradold, 9 * N); cp(d.sg, d.s_sg, 6 * N);
+            cp(d.edotp, d.s_edotp, 6 * N); cp(d.gamdot, d.s_gamdot, ns * N); cp(d.trialtau, d.s_trialtau, 2 * ns * N);
+        }
+    }
+
+    // ------------------------------------------------------------ state_6x6_evpsc (various_functions.f90:1638-1705)
+    void state_6x6(const int* idsim, double* dbar, const int* iscau, double* sbar, const double* xm, const double* devp0,
+                   double* scauchy, double* dsim) {
+        double profac[6], dbarv[6], sbarv[6], devp0v[6], aux6[6], aux6a[6], a4[81], xmv[36], a33[9], A[36];
+        for (int i = 1; i <= 6; i++) profac[i - 1] = 1.0 + (i / 4);
+        for (int i = 0; i < 6; i++) {
+            dbarv[i] = dsim[3 * ijv_a(i) + ijv_b(i)];
+            sbarv[i] = scauchy[3 * ijv_a(i) + ijv_b(i)];
+        }
+        b66_to_t4(xm, a4);
+        for (int i = 0; i < 6; i++)
+            for (int j = 0; j < 6; j++) xmv[6 * i + j] = a4[(3 * ijv_a(i) + ijv_b(i)) * 9 + 3 * ijv_a(j) + ijv_b(j)];
+        b6_to_t2(devp0, a33);
+        for (int i = 0; i < 6; i++) devp0v[i] = a33[3 * ijv_a(i) + ijv_b(i)];
+        for (int i = 0; i < 6; i++) aux6[i] = dbarv[i] - devp0v[i];
+        for (int i = 0; i < 6; i++) {
+            aux6a[i] = -1.0 * idsim[i] * aux6[i];
+            for (int j = 0; j < 6; j++) {
+                aux6a[i] = aux6a[i] + xmv[6 * i + j] * iscau[j] * sbarv[j] * profac[j];
+                A[6 * i + j] = iscau[j] * (i == j ? 1 : 0) - idsim[j] * xmv[6 * i + j] * profac[j];
+            }
+        }
+        int piv[6];
+        if (lu_factor(A, 6, piv) != 0) throw SolveError("Failed system solve in lu_eqsystem (state_6x6_evpsc)", -3);
+        lu_solve(A, 6, piv, aux6a);
+        for (int i = 0; i < 6; i++) {
+            aux6[i] = idsim[i] * aux6[i] + iscau[i] * aux6a[i];
+            sbarv[i] = iscau[i] * sbarv[i] + idsim[i] * aux6a[i];
+        }
+        for (int i = 0; i < 6; i++) dbarv[i] = aux6[i] + devp0v[i];
+        for (int i = 0; i < 6; i++) {
+            dsim[3 * ijv_a(i) + ijv_b(i)] = dbarv[i];
+            dsim[3 * ijv_b(i) + ijv_a(i)] = dbarv[i];
+            scauchy[3 * ijv_a(i) + ijv_b(i)] = sbarv[i];
+            scauchy[3 * ijv_b(i) + ijv_a(i)] = sbarv[i];
+        }
+        t2_to_b6(dsim, dbar);
+        t2_to_b6(scauchy, sbar);
+    }
+
+    // ------------------------------------------------------------ calc_velgradavg_corr tail (various_functions.f90:1575-1631)
+    void velgradavg_corr(const double* sgsol6) {
+        ProcessData& p = P();
+        s6_to_t2(sgsol6, sgavg);
+        for (int c = 0; c < 9; c++) sgavgsol[c] = sgavg[c] / wphcsol;
+        svmavg = vm_stress(sgavg);
+        double a33[9];
+        for (int i = 0; i < 6; i++) {
+            int ii = ijv_a(i), jj = ijv_b(i);
+            a33[3 * ii + jj] = p.iscau[i] * (p.scauchy[3 * ii + jj] - sgavg[3 * ii + jj]);
+            a33[3 * jj + ii] = p.iscau[i] * (p.scauchy[3 * jj + ii] - sgavg[3 * jj + ii]);
+        }
+        errsbc = frob3(a33);
+        double vsym[9], vasym[9], dbar[6], sbar[6], mev[36], devp0[6];
+        sym33(velgradavg, vsym);
+        antisym33(velgradavg, vasym);
+        t2_to_b6(vsym, dbar);
+        t2_to_b6(sgavg, sbar);
+        t4_to_b66(de_ds, mev);
+        for (int i = 0; i < 6; i++) {
+            double s = 0.0;
+            for (int j = 0; j < 6; j++) s += mev[6 * i + j] * sbar[j];
+            devp0[i] = dbar[i] - s;
+        }
+        state_6x6(p.idsim, dbar, p.iscau, sbar, mev, devp0, p.scauchy, p.dsim);
+        double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int ii = 0; ii < 3; ii++)
+            for (int jj = 0; jj < 3; jj++) {
+                if (ii == jj) { w[3 * ii + jj] = 0.0; continue; }
+                const int a = p.iudot[3 * ii + jj], b = p.iudot[3 * jj + ii];
+                if (a == 1 && b == 0) {
+                    w[3 * ii + jj] = p.udot[3 * ii + jj] - p.dsim[3 * ii + jj];
+                    w[3 * jj + ii] = -w[3 * ii + jj];
+                } else if (a == 0 && b == 1) {
+                } else if (a == 1 && b == 1) {
+                    w[3 * ii + jj] = 0.5 * (p.udot[3 * ii + jj] - p.udot[3 * jj + ii]);
+                } else {
+                    w[3 * jj + ii] = 0.0;
+                }
+            }
+        for (int c = 0; c < 9; c++) dvelgradavg[c] = (p.dsim[c] - vsym[c]) + (w[c] - vasym[c]);
+    }
+
+    // ------------------------------------------------------------ one equilibrium iteration (LS-EVPFFT.f90:233-359)
+    void equilibrium_iteration(bool fresh_sgavg) {
+        ProcessData& p = P();
+        if (fresh_sgavg) launch_sgavg(d, st);
+        launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st);
+        launch_fft_y(d, pl2, 9, false, st);
+        launch_fft_z_green(d, pl3, d_c0, d_s0, st);
+        launch_fft_y(d, pl2, 9, true, st);
+        XinvParams xp;
+        std::memcpy(xp.dvelgradavg, dvelgradavg, sizeof(xp.dvelgradavg));
+        if (inv3(dinvc, xp.dinv) != 0) throw SolveError("Singular matrix in lu_inverse (correction_to_current)", -3);
+        launch_fft_x_inv(d, pl1, 0, xp, st);
+        CorrParams cp;
+        cp.mix = mix;
+        cp.Lscale = std::max(lvmavg, EVP_TINY);
+        cp.do_mix = do_mix ? 1 : 0;
+        cp.kinematic = kinematic ? 1 : 0;
+        launch_corr(d, cp, st);
+        NewtonParams np;
+        np.tdot = p.tdot;
+        np.error = p.error;
+        np.erroral = p.erroral;
+        np.complgas = dk.complgas;
+        np.modal = modal ? 1 : 0;
+        np.thermo = (imicro == 1 && p.ithermo == 1) ? 1 : 0;
+        np.iuphard = p.iuphard;
+        launch_newton(d, np, st);
+        CK(cudaGetLastError());
+        fetch_red();
+        const double* cr = h_red + OFF_CORR;
+        for (int c = 0; c < 9; c++) {
+            velgradavg[c] = cr[c];
+            velgradavggas[c] = cr[9 + c];
+            velgradavgsol[c] = cr[18 + c];
+        }
+        if (wphcgas > 0.0)
+            for (int c = 0; c < 9; c++) velgradavggas[c] /= wphcgas;
+        for (int c = 0; c < 9; c++) velgradavgsol[c] /= wphcsol;
+        if (!kinematic) {
+            const double dls = cr[28] > 0.0 ? std::sqrt(cr[27] / cr[28]) : 0.0;
+            const double dlg = cr[30] > 0.0 ? std::sqrt(cr[29] / cr[30]) : 0.0;
+            const double dl = std::max(dls, dlg);
+            mix = std::max(1.0e-8, std::min(1.0, 5.0e-2 / std::max(dl, 5.0e-2)));
+        }
+        const double* nw = h_red + OFF_NEWTON;
+        errs = nw[0];
+        erre = nw[1];
+        if (erre < 0 || errs < 0) throw SolveError("ERRE/ERRS negative -> convergence failed!", -4);
+        erre = std::sqrt(erre);
+        errs = std::sqrt(errs);
+        velgradavg_corr(nw + 2);
+        erre = erre / lvmavg;
+        errs = errs / svmavg;
+        errsbc = errsbc / svmavg;
+    }
+
+    int kinematic_substep(double tdot_step, double& min_detF) {
+        launch_kinematic(d, tdot_step, st);
+        CK(cudaGetLastError());
+        fetch_red();
+        const double mv = h_red[OFF_KIN], mr = h_red[OFF_KIN + 1], ms = h_red[OFF_KIN + 2];
+        min_detF = -h_red[OFF_KIN + 3];
+        const double worst = std::max(std::max(1.0, mv / 5.0e-2), std::max(mr / 2.0, ms / 5.0e-2));
+        return std::max(1, (int)std::ceil(worst));
+    }
+
+    // ------------------------------------------------------------ one macrostep (LS-EVPFFT.f90:199-588)
+    bool macrostep() {
+        while (ipr == 0 || imicro >= P().nsteps) {
+            if (ipr >= dk.nproc) { finished = true; return false; }
+            ipr++;
+            nconverged = 0;
+            kinematic = (P().iscau[2] == 0);
+            tdot_plan = P().tdot;
+            proc_time_target = (double)P().nsteps * tdot_plan;
+            proc_time_done = 0.0;
+            imicro = 0;
+        }
+        ProcessData& p = P();
+        imicro++;
+        CK(cudaEventRecord(ev0, st));
+        if (p.ictrl == -1) {
+            const double remaining = std::max(0.0, proc_time_target - proc_time_done);
+            p.tdot = (remaining > 0.0) ? std::min(tdot_plan, remaining) : tdot_plan;
+        }
+        snapshot(true);
+        bool did_converge = false, accept_step = false;
+        const int do_schmid = ((imicro == 1 && ipr == 1) || p.iupdate == 1) ? 1 : 0;
+        if (modal) {  // form_G: only the real-space origin value is needed (Gamma is applied on the fly)
+            launch_goperr0(d, d_c0, d_s0, st);
+            fetch_red();
+            for (int c = 0; c < 81; c++) goperr0[c] = h_red[OFF_G0 + c] / (double)d.N;
+            CK(cudaMemcpyAsync(d_g0, goperr0, sizeof(goperr0), cudaMemcpyHostToDevice, st));
+        }
+        launch_prologue(d, d_c0, d_g0, do_schmid, modal ? 1 : 0, st);
+        iter = 0;
+        bool fresh = true;
+        while (!(did_converge || accept_step)) {
+            if (iter == 0) {
+                if (dk.has_gas) launch_gas_compl(d, p.tdot, dk.complgas, modal ? 1 : 0, st);
+                std::memset(dvelgradavg, 0, sizeof(dvelgradavg));
+                edotvmmx = 0;
+                mix = 1.0;
+                erre = 2.0 * p.error; errs = 2.0 * p.error; errsbc = 2.0 * p.error;
+                fresh = true;
+            }
+            iter++;
+            total_iters++;
+            if (verbose) {
+                std::printf("\rMACROSTEP=%d SimTime=%.0fs PROC=%d STEP=%d TDOT=%.0fs ITER=%d", imacroloop, sim_time, ipr, imicro, p.tdot, iter);
+                std::fflush(stdout);
+            }
+            equilibrium_iteration(fresh);
+            fresh = false;
+            if (p.ictrl == 0) {
+                double vs[9];
+                sym33(velgradavg, vs);
+                p.tdot = p.devmapp / vm_strain(vs);
+                p.tdotref = p.tdot;
+            }
+            if (errs <= p.error && erre <= p.error && errsbc <= p.error) did_converge = true;
+            if (p.ictrl == -1) {
+                if (p.tdot > p.tdotmin) {
+                    double md;
+                    if (!did_converge && iter == p.itmax) {
+                        double tdot = p.tdot;
+                        int nsub = kinematic_substep(tdot, md);
+                        tdot = tdot / nsub;
+                        tdot = std::max(p.tdotmin, std::min(tdot, 0.5 * p.tdot));
+                        nsub = (int)std::ceil(p.tdot / tdot);
+                        if (nsub > 1) {
+                            const double remaining = std::max(0.0, proc_time_target - proc_time_done);
+                            tdot_plan = tdot;
+                            const int nnew = (imicro - 1) + (int)std::ceil(remaining / tdot_plan);
+                            total_macrosteps += nnew - p.nsteps;
+                            p.nsteps = nnew;
+                            p.tdot = std::min(tdot_plan, remaining);
+                            nconverged = 0;
+                            iter = 0;
+                            snapshot(false);
+                        }
+                    } else if (did_converge) {
+                        double tdot = p.tdot;
+                        int nsub = kinematic_substep(tdot, md);
+                        tdot = tdot / nsub;
+                        if (md <= 1.0e-3) tdot = std::max(p.tdotmin, std::min(tdot, 0.5 * p.tdot));
+                        else tdot = std::max(p.tdotmin, tdot);
+                        nsub = (int)std::ceil(p.tdot / tdot);
+                        if (nsub > 1) {
+                            const double remaining = std::max(0.0, proc_time_target - proc_time_done);
+                            tdot_plan = tdot;
+                            const int nnew = (imicro - 1) + (int)std::ceil(remaining / tdot_plan);
+                            total_macrosteps += nnew - p.nsteps;
+                            p.nsteps = nnew;
+                            p.tdot = std::min(tdot_plan, remaining);
+                            did_converge = false;
+                            nconverged = 0;
+                            iter = 0;
+                            mix = 1.0;
+                            snapshot(false);
+                        }
+                    }
+                } else if (iter == p.itmax) {
+                    accept_step = true;
+                }
+            }
+            if (iter >= 100000) throw SolveError("equilibrium iteration did not converge", -4);
+        }
+        const int iter_done = iter;
+        // commit + large-strain updates (LS-EVPFFT.f90:432-458)
+        if (p.iupdate == 1) {  // update_grid_velgrad_node reads L and F before update_defgrad changes F
+            launch_fft_x_fwd(d, pl1, 1, 0, st);
+            launch_fft_y(d, pl2, 9, false, st);
+            launch_fft_z_integ(d, pl3, p.igamma, st);
+            launch_fft_y(d, pl2, 3, true, st);
+            XinvParams xp{};
+            launch_fft_x_inv(d, pl1, 1, xp, st);
+            launch_cell2node(d, p.tdot, p.igamma, st);
+        }
+        Upd1Params u1;
+        u1.tdot = p.tdot;
+        u1.iupdate = p.iupdate;
+        launch_upd1(d, u1, st);
+        if (p.iupdate == 1) {
+            Upd2Params u2;
+            std::memcpy(u2.velgradavg, velgradavg, sizeof(u2.velgradavg));
+            launch_upd2(d, u2, st);
+        }
+        Upd3Params u3;
+        u3.tdot = p.tdot;
+        u3.iupdate = p.iupdate;
+        u3.iuphard = p.iuphard;
+        u3.vlast = vlast;
+        launch_upd3(d, u3, st);
+        // averages that only depend on host values
+        double vsym[9];
+        sym33(velgradavg, vsym);
+        lvmavg = vm_strain(velgradavg);
+        dvmavg = vm_strain(vsym);
+        evmavg = evmavg + dvmavg * p.tdot;
+        const double Lref = std::max(lvmavg, EVP_TINY);
+        launch_diag(d, std::max(1.0e-12 * Lref, EVP_TINY), st);
+        // time bookkeeping and the tdot ramp are host-only; they fix the tdot calc_c0 sees
+        const double tdot_used = p.tdot;
+        const double tdotref_used = p.tdotref;
+        if (p.ictrl == -1) {
+            proc_time_done += tdot_used;
+            p.tdot = tdot_plan;
+        }
+        sim_time += tdot_used;
+        if (p.ictrl == -1) {
+            if (tdot_plan < p.tdotref && nconverged >= 5) {
+                nconverged = 0;
+                tdot_plan = std::min(2.0 * tdot_plan, p.tdotref);
+                const double remaining = std::max(0.0, proc_time_target - proc_time_done);
+                const int left = (int)std::ceil(remaining / tdot_plan);
+                const int nnew = imicro + left;
+                total_macrosteps += nnew - p.nsteps;
+                p.nsteps = nnew;
+                p.tdot = (remaining > 0.0) ? std::min(tdot_plan, remaining) : tdot_plan;
+            }
+        } else if (p.tdot < p.tdotref && nconverged >= 5) {
+            nconverged = 0;
+            const double tdot = p.tdot;
+            p.tdot = std::min(2.0 * p.tdot, p.tdotref);
+            int left = p.nsteps - imicro;
+            left = (int)std::ceil((double)left * tdot / p.tdot);
+            total_macrosteps += left - (p.nsteps - imicro);
+            p.nsteps = imicro + left;
+        }
+        const bool conv_for_count = did_converge;
+        launch_c0(d, p.tdot, p.tdotref, st);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev1, st));
+        fetch_red();
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) gpu_ms += ms;
+        // update_defgrad averages (host side of various_functions.f90:2250-2266)
+        const double* u1o = h_red + OFF_UPD1;
+        edotvmmx = u1o[39];
+        if (p.iupdate == 1) {
+            const double dav = u1o[38];
+            for (int c = 0; c < 9; c++) { defgradavg[c] = u1o[c]; dinvc[c] = u1o[9 + c] / dav; }
+            wphcsol = u1o[36] / dav;
+            wphcgas = u1o[37] / dav;
+            for (int c = 0; c < 9; c++) dinvcs[c] = u1o[18 + c] / dav / wphcsol;
+            if (wphcgas > 0.0) for (int c = 0; c < 9; c++) dinvcg[c] = u1o[27 + c] / dav / wphcgas;
+            else for (int c = 0; c < 9; c++) dinvcg[c] = (c % 4 == 0) ? 1.0 : 0.0;
+        }
+        // macro averages (LS-EVPFFT.f90:465-523)
+        const double* r3 = h_red + OFF_UPD3;
+        double ep6[6], ea6[6], el6[6], ed6[6], ss6[6];
+        for (int c = 0; c < 6; c++) {
+            ep6[c] = r3[c] / wphcsol;
+            ea6[c] = r3[6 + c] / wphcsol;
+            ed6[c] = r3[12 + c] / wphcsol;
+            ss6[c] = r3[18 + c] / wphcsol;
+            // eelavg = eavg + (disgradsym - ept) * wgtc of the last solid voxel (LS-EVPFFT.f90:482-483)
+            el6[c] = (r3[6 + c] + (r3[30 + c] - r3[36 + c]) * r3[42]) / wphcsol;
+        }
+        s6_to_t2(ep6, epavg); s6_to_t2(ea6, eavg); s6_to_t2(el6, eelavg); s6_to_t2(ed6, edotpavg); s6_to_t2(ss6, sgsolavg);
+        const double nsolid = r3[25], nsys_solid = r3[27];
+        const double gammaavg = nsolid > 0.0 ? r3[24] / nsolid : 0.0;
+        const double gavg = nsys_solid > 0.0 ? r3[26] / nsys_solid : 0.0;
+        const double geffavg = r3[28] > 0.0 ? r3[29] / r3[28] : gavg;
+        evmpavg = vm_strain(epavg);
+        dvmpavg = vm_strain(edotpavg);
+        if (p.iwfields == 1) {
+            const int aw = std::abs(p.iwstep);
+            const bool due = (aw != 0 && imicro % aw == 0) || (p.iwstep < 0 && imicro == p.nsteps);
+            if (due && write_files) write_vtk(imacroloop);
+        }
+        finish_diag();
+        dg.erre = erre; dg.errs = errs; dg.errsbc = errsbc;
+        dg.tdotref = tdotref_used;
+        dg.s33_target = p.scauchy[8];
+        dg.s33 = sgavg[8];
+        dg.s33_sol = sgsolavg[8];
+        dg.devm_inc_max = edotvmmx * tdot_used;
+        wall_time = (double)(std::time(nullptr) - start);
+        write_rows(iter_done, imacroloop, ipr, sim_time, wall_time, tdot_used, dg.tdotref, gammaavg, gavg, geffavg);
+        if (conv_for_count) nconverged++;
+        finish_c0(p);
+        imacroloop++;
+        macrosteps_done++;
+        return true;
+    }
+
+    void finish_diag() {
+        const double* r = h_red + OFF_DIAG;
+        const long long n1 = d.n1, n2 = d.n2;
+        dg.dl_rms = r[1] > 0 ? std::sqrt(r[0] / r[1]) : 0.0;
+        dg.dl_rms_sol = r[3] > 0 ? std::sqrt(r[2] / r[3]) : 0.0;
+        dg.dl_rms_gas = r[5] > 0 ? std::sqrt(r[4] / r[5]) : 0.0;
+        dg.dl_max = r[6]; dg.dl_max_sol = r[7]; dg.dl_max_gas = r[8];
+        dg.volinc_sol = r[9]; dg.volinc_gas = r[10]; dg.rot_sol = r[11]; dg.rot_gas = r[12];
+        dg.stretch_sol = r[13]; dg.stretch_gas = r[14];
+        dg.cond_sol = r[15]; dg.cond_gas = r[16]; dg.cond_cgas = r[17];
+        dg.detF_min = -r[18];
+        auto idx = [&](double vv, int* out) {
+            if (vv < 0) { out[0] = out[1] = out[2] = 0; return; }
+            long long v = (long long)vv;
+            out[0] = (int)(v % n1) + 1; out[1] = (int)((v / n1) % n2) + 1; out[2] = (int)(v / (n1 * n2)) + 1;
+        };
+        dg.detF_min_sol = r[19];
+        idx(r[20], dg.imin_sol);
+        dg.detF_min_gas = r[21];
+        idx(r[22], dg.imin_gas);
+        if (dg.detF_min >= EVP_HUGE * 0.5) dg.detF_min = 0.0;
+        if (dg.detF_min_sol >= EVP_HUGE * 0.5) dg.detF_min_sol = 0.0;
+        if (dg.detF_min_gas >= EVP_HUGE * 0.5) dg.detF_min_gas = 0.0;
+        dg.dvelgradavg_mag = frob3(dvelgradavg);
+        dg.detF_min_prev = dg.detF_min;
+        dg.detF_min_sol_rel = safe_rel(dg.detF_min_sol, dg.detF_min_sol_prev);
+        dg.detF_min_sol_prev = dg.detF_min_sol;
+        dg.detF_min_gas_rel = safe_rel(dg.detF_min_gas, dg.detF_min_gas_prev);
+        dg.detF_min_gas_prev = dg.detF_min_gas;
+        dg.volinc_sol_rel = safe_rel(dg.volinc_sol, dg.volinc_sol_prev); dg.volinc_sol_prev = dg.volinc_sol;
+        dg.volinc_gas_rel = safe_rel(dg.volinc_gas, dg.volinc_gas_prev); dg.volinc_gas_prev = dg.volinc_gas;
+        dg.stretch_sol_rel = safe_rel(dg.stretch_sol, dg.stretch_sol_prev); dg.stretch_sol_prev = dg.stretch_sol;
+        dg.stretch_gas_rel = safe_rel(dg.stretch_gas, dg.stretch_gas_prev); dg.stretch_gas_prev = dg.stretch_gas;
+    }
+
+    void finish_c0(const ProcessData& p) {  // calc_c0 tail (various_functions.f90:2633-2647)
+        const double* r = h_red + OFF_C0;
+        double dsde[81], dP[36], a[36], ai[36];
+        for (int c = 0; c < 81; c++) dsde[c] = r[c] / wphcsol;
+        for (int c = 0; c < 36; c++) dP[c] = r[81 + c] / wphsol;
+        t4_to_b66(dsde, a);
+        std::memcpy(ai, a, sizeof(a));
+        if (lu_inverse(ai, 6) != 0) throw SolveError("Singular matrix in lu_inverse (calc_c0)", -3);
+        b66_to_t4(ai, de_ds);
+        for (int c = 0; c < 36; c++) { c066[c] = dP[c] * p.xc0; a[c] = dP[c] * p.xc0; }
+        if (lu_inverse(a, 6) != 0) throw SolveError("Singular matrix in lu_inverse (calc_c0)", -3);
+        b66_to_t4(c066, c0);
+        b66_to_t4(a, s0);
+        upload_c0();
+    }
+
+    // ------------------------------------------------------------ outputs
+    std::string csv_path(const char* name) const {
+        if (!outdir.empty() && outdir.back() == '/') return outdir + name;
+        return outdir + "/" + name;
+    }
+    void write_headers() {
+        FILE* f = std::fopen(csv_path("diagnostics.csv").c_str(), "w");
+        if (!f) throw SolveError("write_diagnostics: failed to open diagnostics.csv for writing", -5);
+        std::fputs("iter,macrostep,ipr,sim_time,wall_time,tdot,vm_max_inc,tdotref,erre,errs,errsbc,s33_target,s33,s33_sol,"
+                   "detF_min_sol,detF_min_gas,detF_min_sol_rel,detF_min_gas_rel,volinc_max_sol,volinc_max_gas,volinc_max_sol_rel,"
+                   "volinc_max_gas_rel,stretchinc_max_sol,stretchinc_max_gas,stretchinc_max_sol_rel,stretchinc_max_gas_rel,"
+                   "rotang_max_sol,rotang_max_gas,dL_step_rms_sol,dL_step_rms_gas,dL_step_rms,dL_step_max_sol,dL_step_max_gas,"
+                   "dL_step_max,dvelgradavg_mag,cond_c066mod_max_sol,cond_c066mod_max_gas,cond_cgas_max,imin_sol_i,imin_sol_j,"
+                   "imin_sol_k,imin_gas_i,imin_gas_j,imin_gas_k\n", f);
+        std::fclose(f);
+        f = std::fopen(csv_path("results.csv").c_str(), "w");
+        if (!f) throw SolveError("results: failed to open results.csv for writing", -5);
+        std::fputs("iter,macrostep,ipr,sim_time,wall_time,tdot,tdot_ref,eav11,eav22,eav33,eav23,eav13,eav12,sav11,sav22,sav33,"
+                   "sav23,sav13,sav12,epav11,epav22,epav33,epav23,epav13,epav12,eelav11,eelav22,eelav33,eelav23,eelav13,"
+                   "eelav12,vgrad11,vgrad22,vgrad33,vgrad23,vgrad13,vgrad12,edotp11,edotp22,edotp33,edotp23,edotp13,edotp12,"
+                   "evm,evmp,dvm,dvmp,svm,gamma,g,geff\n", f);
+        std::fclose(f);
+    }
+    void write_rows(int it, int imac, int ip, double st_, double wt, double tdot, double tdotref, double gamma, double g, double geff) {
+        double* R = last_results;
+        int c = 0;
+        R[c++] = it; R[c++] = imac; R[c++] = ip; R[c++] = st_; R[c++] = wt; R[c++] = tdot; R[c++] = tdotref;
+        auto put6 = [&](const double* m) { R[c++] = m[0]; R[c++] = m[4]; R[c++] = m[8]; R[c++] = m[5]; R[c++] = m[2]; R[c++] = m[1]; };
+        put6(eavg); put6(sgsolavg); put6(epavg); put6(eelavg); put6(velgradavg); put6(edotpavg);
+        R[c++] = evmavg; R[c++] = evmpavg; R[c++] = dvmavg; R[c++] = dvmpavg; R[c++] = svmavg; R[c++] = gamma; R[c++] = g; R[c++] = geff;
+        double D[44] = {(double)it, (double)imac, (double)ip, st_, wt, tdot, dg.devm_inc_max, dg.tdotref, dg.erre, dg.errs, dg.errsbc,
+                        dg.s33_target, dg.s33, dg.s33_sol, dg.detF_min_sol, dg.detF_min_gas, dg.detF_min_sol_rel, dg.detF_min_gas_rel,
+                        dg.volinc_sol, dg.volinc_gas, dg.volinc_sol_rel, dg.volinc_gas_rel, dg.stretch_sol, dg.stretch_gas,
+                        dg.stretch_sol_rel, dg.stretch_gas_rel, dg.rot_sol, dg.rot_gas, dg.dl_rms_sol, dg.dl_rms_gas, dg.dl_rms,
+                        dg.dl_max_sol, dg.dl_max_gas, dg.dl_max, dg.dvelgradavg_mag, dg.cond_sol, dg.cond_gas, dg.cond_cgas,
+                        (double)dg.imin_sol[0], (double)dg.imin_sol[1], (double)dg.imin_sol[2], (double)dg.imin_gas[0],
+                        (double)dg.imin_gas[1], (double)dg.imin_gas[2]};
+        std::memcpy(last_diag, D, sizeof(D));
+        if (!write_files) return;
+        std::string line;
+        for (int q = 0; q < 44; q++) {
+            line += (q < 3 || q >= 38) ? std::to_string((long long)D[q]) : g0(D[q]);
+            line += (q == 43) ? '\n' : ',';
+        }
+        FILE* f = std::fopen(csv_path("diagnostics.csv").c_str(), "a");
+        if (!f) throw SolveError("write_diagnostics: failed to open diagnostics.csv for append", -5);
+        std::fputs(line.c_str(), f);
+        std::fclose(f);
+        line.clear();
+        for (int q = 0; q < 53; q++) {
+            line += (q < 3) ? std::to_string((long long)R[q]) : g0(R[q]);
+            line += (q == 52) ? '\n' : ',';
+        }
+        f = std::fopen(csv_path("results.csv").c_str(), "a");
+        if (!f) throw SolveError("write_results: failed to open results.csv for append", -5);
+        std::fputs(line.c_str(), f);
+        std::fclose(f);
+    }
+
+    std::vector<double> field_host(double* dp, size_t n) {
+        std::vector<double> h(n);
+        CK(cudaMemcpyAsync(h.data(), dp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync();
+        return h;
+    }
+    void write_vtk(int istp) {  // write_vtk_cell (IO_functions.f90:945-1235)
+        const long long N = d.N;
+        const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+        auto xn = field_host(d.xnode, 3 * (size_t)(n1 + 1) * (n2 + 1) * d.n3node);
+        auto gd = field_host(d.gamdot, (size_t)d.nsys * N);
+        auto ga = field_host(d.gacumgr, N);
+        auto fp = field_host(d.Fp, 9 * N);
+        auto sg = field_host(d.sg, 6 * N);
+        auto F = field_host(d.F, 9 * N);
+        auto dF = field_host(d.detF, N);
+        auto ep = field_host(d.epvm, N);
+        auto vg = field_host(d.velgrad, 9 * N);
+        char name[64];
+        std::snprintf(name, sizeof(name), "microstr_cell_fields_stp_%05d.vtk", istp);
+        std::string path = outdir + "/" + name;
+        FILE* f = std::fopen(path.c_str(), "w");
+        if (!f) throw SolveError("ioerr in writevtk", -5);
+        std::string o;
+        o.reserve(1 << 20);
+        char b[256];
+        o += "# vtk DataFile Version 3.0\nmicrostructure data\nASCII\nDATASET UNSTRUCTURED_GRID\n";
+        const long long nn1 = n1 + 1, nn2 = n2 + 1;
+        auto nid = [&](int i, int j, int k) { return (long long)i + nn1 * ((long long)j + nn2 * (long long)k); };
+        auto flush = [&]() { std::fwrite(o.data(), 1, o.size(), f); o.clear(); };
+        long long ncell;
+        if (n3 == 1) {
+            std::snprintf(b, sizeof(b), "POINTS%10lld double\n", nn1 * nn2);
+            o += b;
+            for (int j = 0; j < n2 + 1; j++)
+                for (int i = 0; i < n1 + 1; i++) {
+                    long long q = 3 * nid(i, j, 0);
+                    put_e18(o, xn[q]); put_e18(o, xn[q + 1]); put_e18(o, xn[q + 2]);
+                    o += '\n';
+                }
+            ncell = (long long)n1 * n2;
+            std::snprintf(b, sizeof(b), "CELLS%10lld%10lld\n", ncell, ncell * 5);
+            o += b;
+            for (int j = 0; j < n2; j++)
+                for (int i = 0; i < n1; i++) {
+                    std::snprintf(b, sizeof(b), "%10d%10lld%10lld%10lld%10lld\n", 4, nid(i, j, 0), nid(i + 1, j, 0), nid(i, j + 1, 0), nid(i + 1, j + 1, 0));
+                    o += b;
+                }
+            std::snprintf(b, sizeof(b), "CELL_TYPES%10lld\n", ncell);
+            o += b;
+            for (long long c = 0; c < ncell; c++) o += "    8\n";
+        } else {
+            std::snprintf(b, sizeof(b), "POINTS%10lld double\n", nn1 * nn2 * (n3 + 1));
+            o += b;
+            for (int k = 0; k < n3 + 1; k++)
+                for (int j = 0; j < n2 + 1; j++)
+                    for (int i = 0; i < n1 + 1; i++) {
+                        long long q = 3 * nid(i, j, k);
+                        put_e18(o, xn[q]); put_e18(o, xn[q + 1]); put_e18(o, xn[q + 2]);
+                        o += '\n';
+                        if (o.size() > (1 << 20)) flush();
+                    }
+            ncell = N;
+            std::snprintf(b, sizeof(b), "CELLS%10lld%10lld\n", ncell, ncell * 9);
+            o += b;
+            for (int k = 0; k < n3; k++)
+                for (int j = 0; j < n2; j++)
+                    for (int i = 0; i < n1; i++) {
+                        std::snprintf(b, sizeof(b), "%10d%10lld%10lld%10lld%10lld%10lld%10lld%10lld%10lld\n", 8, nid(i, j, k), nid(i + 1, j, k),
+                                      nid(i + 1, j + 1, k), nid(i, j + 1, k), nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1),
+                                      nid(i, j + 1, k + 1));
+                        o += b;
+                        if (o.size() > (1 << 20)) flush();
+                    }
+            std::snprintf(b, sizeof(b), "CELL_TYPES%10lld\n", ncell);
+            o += b;
+            for (long long c = 0; c < ncell; c++) o += "   12\n";
+        }
+        std::snprintf(b, sizeof(b), "CELL_DATA%10lld\nFIELD FieldData%10d\n", ncell, 11);
+        o += b;
+        const int ns = d.nsys;
+        std::snprintf(b, sizeof(b), "gamdot%3d%10lld double\n", ns, ncell);
+        o += b;
+        for (long long v = 0; v < N; v++) {
+            for (int s = 0; s < ns; s++) put_e18(o, gd[s * N + v]);
+            o += '\n';
+            if (o.size() > (1 << 20)) flush();
+        }
+        auto scalar = [&](const char* nm, const std::vector<double>& a) {
+            std::snprintf(b, sizeof(b), "%s%3d%10lld double\n", nm, 1, ncell);
+            o += b;
+            for (long long v = 0; v < N; v++) {
+                put_e18(o, a[v]);
+                o += '\n';
+                if (o.size() > (1 << 20)) flush();
+            }
+        };
+        auto tens9 = [&](const char* nm, const std::vector<double>& a) {  // column-major order
+            std::snprintf(b, sizeof(b), "%s%3d%10lld double\n", nm, 9, ncell);
+            o += b;
+            for (long long v = 0; v < N; v++) {
+                for (int c = 0; c < 3; c++)
+                    for (int r = 0; r < 3; r++) put_e18(o, a[(3 * r + c) * N + v]);
+                o += '\n';
+                if (o.size() > (1 << 20)) flush();
+            }
+        };
+        scalar("gamdot_acum", ga);
+        tens9("def_grad_p", fp);
+        std::snprintf(b, sizeof(b), "stress%3d%10lld double\n", 6, ncell);
+        o += b;
+        for (long long v = 0; v < N; v++) {
+            put_e18(o, sg[0 * N + v]); put_e18(o, sg[1 * N + v]); put_e18(o, sg[2 * N + v]);
+            put_e18(o, sg[5 * N + v]); put_e18(o, sg[3 * N + v]); put_e18(o, sg[4 * N + v]);
+            o += '\n';
+            if (o.size() > (1 << 20)) flush();
+        }
+        std::vector<double> svm(N);
+        for (long long v = 0; v < N; v++) {
+            double s6[6], t[9];
+            for (int c = 0; c < 6; c++) s6[c] = sg[c * N + v];
+            s6_to_t2(s6, t);
+            svm[v] = vm_stress(t);
+        }
+        scalar("svm", svm);
+        tens9("def_grad", F);
+        scalar("det_def_grad", dF);
+        std::snprintf(b, sizeof(b), "gr_id%3d%10lld int\n", 1, ncell);
+        o += b;
+        for (long long v = 0; v < N; v++) {
+            std::snprintf(b, sizeof(b), "%10d\n", dk.grain[v]);
+            o += b;
+            if (o.size() > (1 << 20)) flush();
+        }
+        std::snprintf(b, sizeof(b), "ph_id%3d%10lld int\n", 1, ncell);
+        o += b;
+        for (long long v = 0; v < N; v++) {
+            std::snprintf(b, sizeof(b), "%10d\n", dk.phase_id[v]);
+            o += b;
+            if (o.size() > (1 << 20)) flush();
+        }
+        scalar("epvm", ep);
+        tens9("velgrad", vg);
+        flush();
+        std::fclose(f);
+    }
+
+    long long get_field(const std::string& name, double* out, long long cap) {
+        const long long N = d.N;
+        const int ns = d.nsys;
+        auto soa_to_aos = [&](double* dp, int ncomp, const int* map, int nout) -> long long {
+            if ((long long)nout * N > cap) return -1;
+            auto h = field_host(dp, (size_t)ncomp * N);
+            for (long long v = 0; v < N; v++)
+                for (int c = 0; c < nout; c++) out[nout * v + c] = h[(size_t)map[c] * N + v];
+            return (long long)nout * N;
+        };
+        static const int id9[9] = {0, 1, 2, 3, 4, 5, 6, 7, 8};
+        static const int s6to9[9] = {0, 5, 4, 5, 1, 3, 4, 3, 2};  // (11,22,33,23,13,12) -> row-major 3x3
+        if (name == "sg") return soa_to_aos(d.sg, 6, s6to9, 9);
+        if (name == "sgt") return soa_to_aos(d.sgt, 6, s6to9, 9);
+        if (name == "edotp") return soa_to_aos(d.edotp, 6, s6to9, 9);
+        if (name == "ept") return soa_to_aos(d.ept, 6, s6to9, 9);
+        if (name == "disgradsym") return soa_to_aos(d.disgradsym, 6, s6to9, 9);
+        if (name == "velgrad") return soa_to_aos(d.velgrad, 9, id9, 9);
+        if (name == "velgradold") return soa_to_aos(d.velgradold, 9, id9, 9);
+        if (name == "dvelgradref") return soa_to_aos(d.dvr, 9, id9, 9);
+        if (name == "defgrad") return soa_to_aos(d.F, 9, id9, 9);
+        if (name == "defgradinv") return soa_to_aos(d.Finv, 9, id9, 9);
+        if (name == "defgrade") return soa_to_aos(d.Fe, 9, id9, 9);
+        if (name == "defgradp") return soa_to_aos(d.Fp, 9, id9, 9);
+        if (name == "detF") return soa_to_aos(d.detF, 1, id9, 1);
+        if (name == "wgtc") return soa_to_aos(d.wgtc, 1, id9, 1);
+        if (name == "gacumgr") return soa_to_aos(d.gacumgr, 1, id9, 1);
+        if (name == "epvm") return soa_to_aos(d.epvm, 1, id9, 1);
+        std::vector<int> m(72);
+        for (int c = 0; c < 72; c++) m[c] = c;
+        if (name == "gamdot") return soa_to_aos(d.gamdot, ns, m.data(), ns);
+        if (name == "crss") return soa_to_aos(d.crss, 2 * ns, m.data(), 2 * ns);
+        if (name == "trialtau") return soa_to_aos(d.trialtau, 2 * ns, m.data(), 2 * ns);
+        if (name == "sch") return soa_to_aos(d.sch, 5 * ns, m.data(), 5 * ns);
+        if (name == "c066mod") return soa_to_aos(d.c066mod, 36, m.data(), 36);
+        if (name == "sg66") return soa_to_aos(d.sg66, 36, m.data(), 36);
+        if (name == "xnode") {
+            long long n = 3LL * (d.n1 + 1) * (d.n2 + 1) * d.n3node;
+            if (n > cap) return -1;
+            CK(cudaMemcpyAsync(out, d.xnode, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync();
+            return n;
+        }
+        return -2;
+    }
+};
+
+}  // namespace evp
+
+using evp::SolveError;
+using evp::Solver;
+
+struct evp_solve {
+    Solver s;
+};
+
+static int fail(const std::string& m, int code) {
+    evp::g_last_error = m;
+    return code;
+}
+
+extern "C" {
+
+int evp_version(void) { return 1; }
+
+const char* evp_last_error(void) { return evp::g_last_error.c_str(); }
+
+int evp_open(const char* fft_in, const char* out_dir, int mix, int modal, int flags, evp_solve** out) {
+    if (!fft_in || !out) return fail("evp_open: null argument", -7);
+    *out = nullptr;
+    evp_solve* h = new evp_solve();
+    try {
+        h->s.open(fft_in, out_dir ? out_dir : "", mix, modal, flags);
+    } catch (SolveError& e) {
+        delete h;
+        return fail(e.what(), e.code);
+    } catch (std::exception& e) {
+        delete h;
+        return fail(e.what(), -1);
+    }
+    *out = h;
+    return 0;
+}
+
+int evp_advance(evp_solve* h, int nmacro, int* done) {
+    if (!h) return fail("evp_advance: null handle", -7);
+    int n = 0;
+    try {
+        for (int i = 0; i < nmacro; i++) {
+            if (!h->s.macrostep()) break;
+            n++;
+        }
+    } catch (SolveError& e) {
+        if (done) *done = n;
+        return fail(e.what(), e.code);
+    } catch (std::exception& e) {
+        if (done) *done = n;
+        return fail(e.what(), -1);
+    }
+    if (done) *done = n;
+    return 0;
+}
+
+int evp_get_field(evp_solve* h, const char* name, double* host_out, long long capacity, long long* written) {
+    if (!h || !name || !host_out) return fail("evp_get_field: null argument", -7);
+    try {
+        long long n = h->s.get_field(name, host_out, capacity);
+        if (n == -2) return fail(std::string("evp_get_field: unknown field ") + name, -7);
+        if (n < 0) return fail("evp_get_field: buffer too small", -7);
+        if (written) *written = n;
+    } catch (SolveError& e) {
+        return fail(e.what(), e.code);
+    }
+    return 0;
+}
+
+int evp_last_rows(evp_solve* h, double* r53, double* d44) {
+    if (!h) return fail("evp_last_rows: null handle", -7);
+    if (r53) std::memcpy(r53, h->s.last_results, sizeof(h->s.last_results));
+    if (d44) std::memcpy(d44, h->s.last_diag, sizeof(h->s.last_diag));
+    return 0;
+}
+
+int evp_stats(evp_solve* h, evp_report* r) {
+    if (!h || !r) return fail("evp_stats: null argument", -7);
+    r->status = 0;
+    r->macrosteps = h->s.macrosteps_done;
+    r->equilibrium_iters = h->s.total_iters;
+    r->voxel_iters = h->s.total_iters * h->s.d.N;
+    r->wall_s = 0.0;
+    r->gpu_s = h->s.gpu_ms * 1e-3;
+    r->n1 = h->s.d.n1; r->n2 = h->s.d.n2; r->n3 = h->s.d.n3;
+    return 0;
+}
+
+int evp_close(evp_solve* h) {
+    delete h;
+    return 0;
+}
+
+int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const char* fftw_save, int mix, int modal, evp_report* report) {
+    (void)nthreads;
+    (void)fftw_save;
+    auto t0 = std::chrono::steady_clock::now();
+    evp_solve* h = nullptr;
+    int rc = evp_open(fft_in, out_dir, mix, modal, EVP_WRITE_FILES, &h);
+    if (rc != 0) {
+        if (report) { std::memset(report, 0, sizeof(*report)); report->status = rc; }
+        return rc;
+    }
+    int done = 0;
+    while (true) {
+        rc = evp_advance(h, 1, &done);
+        if (rc != 0 || done == 0) break;
+    }
+    if (report) {
+        evp_stats(h, report);
+        report->status = rc;
+        report->wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    evp_close(h);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+"""Python front end of the B200 LS-EVPFFT solver.
+
+Mirrors the reference's solver interface: the executable ``lsevpfft/LS-EVPFFT``
+(flags of ``lsevpfft/src/LS-EVPFFT.f90:87-142``) as launched by
+``utils/run.py:169-196`` (``run_solver``), and the files it writes.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+
+RESULTS_COLS = (
+    "iter,macrostep,ipr,sim_time,wall_time,tdot,tdot_ref,eav11,eav22,eav33,eav23,eav13,eav12,sav11,sav22,sav33,"
+    "sav23,sav13,sav12,epav11,epav22,epav33,epav23,epav13,epav12,eelav11,eelav22,eelav33,eelav23,eelav13,"
+    "eelav12,vgrad11,vgrad22,vgrad33,vgrad23,vgrad13,vgrad12,edotp11,edotp22,edotp33,edotp23,edotp13,edotp12,"
+    "evm,evmp,dvm,dvmp,svm,gamma,g,geff").split(",")
+
+DIAG_COLS = (
+    "iter,macrostep,ipr,sim_time,wall_time,tdot,vm_max_inc,tdotref,erre,errs,errsbc,s33_target,s33,s33_sol,"
+    "detF_min_sol,detF_min_gas,detF_min_sol_rel,detF_min_gas_rel,volinc_max_sol,volinc_max_gas,volinc_max_sol_rel,"
+    "volinc_max_gas_rel,stretchinc_max_sol,stretchinc_max_gas,stretchinc_max_sol_rel,stretchinc_max_gas_rel,"
+    "rotang_max_sol,rotang_max_gas,dL_step_rms_sol,dL_step_rms_gas,dL_step_rms,dL_step_max_sol,dL_step_max_gas,"
+    "dL_step_max,dvelgradavg_mag,cond_c066mod_max_sol,cond_c066mod_max_gas,cond_cgas_max,imin_sol_i,imin_sol_j,"
+    "imin_sol_k,imin_gas_i,imin_gas_j,imin_gas_k").split(",")
+
+WRITE_FILES = 1
+VERBOSE = 2
+
+
+def run_solver(fft_in, out_dir="evpfft_outputs/", nthreads=0, fftw_save="", mix=1, modal=1) -> _lib.Report:
+    """One whole solve, as one ``LS-EVPFFT --in ... --out ...`` process would do it.
+
+    Raises ``EvpError`` with the library's status code on failure."""
+    L = _lib.load()
+    rep = _lib.Report()
+    rc = L.evp_solve_file(str(fft_in).encode(), str(out_dir).encode(), int(nthreads), str(fftw_save).encode(), int(mix),
+                          int(modal), ctypes.byref(rep))
+    _lib.check(rc)
+    return rep
+
+
+class Solve:
+    """A device-resident solve advanced macrostep by macrostep."""
+
+    def __init__(self, fft_in, out_dir="", mix=1, modal=1, write_files=False, verbose=False):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        flags = (WRITE_FILES if write_files else 0) | (VERBOSE if verbose else 0)
+        _lib.check(L.evp_open(str(fft_in).encode(), str(out_dir).encode(), int(mix), int(modal), flags, ctypes.byref(h)))
+        self._h = h
+        rep = self.stats()
+        self.shape = (rep.n1, rep.n2, rep.n3)
+        self.nvox = rep.n1 * rep.n2 * rep.n3
+
+    def advance(self, nmacro: int = 1) -> int:
+        done = ctypes.c_int(0)
+        _lib.check(_lib.load().evp_advance(self._h, int(nmacro), ctypes.byref(done)))
+        return done.value
+
+    def run(self) -> list:
+        rows = []
+        while self.advance(1) == 1:
+            rows.append(self.rows()[0])
+        return rows
+
+    def rows(self):
+        r = np.zeros(53)
+        d = np.zeros(44)
+        _lib.load().evp_last_rows(self._h, r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return r, d
+
+    def field(self, name: str) -> np.ndarray:
+        cap = self.nvox * 128 + 3 * (self.shape[0] + 1) * (self.shape[1] + 1) * (self.shape[2] + 1)
+        buf = np.zeros(cap)
+        n = ctypes.c_longlong(0)
+        _lib.check(_lib.load().evp_get_field(self._h, name.encode(), buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap,
+                                             ctypes.byref(n)))
+        return buf[: n.value].copy()
+
+    def stats(self) -> _lib.Report:
+        rep = _lib.Report()
+        _lib.check(_lib.load().evp_stats(self._h, ctypes.byref(rep)))
+        return rep
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().evp_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def load_results(path) -> np.ndarray:
+    """results.csv as a float array (columns RESULTS_COLS)."""
+    return np.loadtxt(Path(path), delimiter=",", skiprows=1, ndmin=2)

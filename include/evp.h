@@ -1,0 +1,76 @@
+/*
+ * evp.h -- C ABI of the B200-native LS-EVPFFT solver (libevp_b200.so).
+ *
+ * The reference solver is the Fortran executable lsevpfft/LS-EVPFFT, launched
+ * as a separate process by utils/run.py:169-196 (run_solver) with
+ *     LS-EVPFFT --nthreads n --in fft.in --out DIR --fftw_save P --mix m --modal a
+ * (flag parsing at lsevpfft/src/LS-EVPFFT.f90:87-142) and talking to its
+ * callers only through files: results.csv (IO_functions.f90:1237-1303),
+ * diagnostics.csv (types.f90:760-834) and VTK (IO_functions.f90:945-1235).
+ * These entry points replace that process.  Plain C types only; the library
+ * owns every device allocation; strings are copied.
+ *
+ * Status codes: 0 ok; -1 deck or input-file error; -2 deck feature not
+ * supported by this build; -3 singular matrix (the reference's `stop 1` in
+ * lu_inverse / lu_eqsystem / dgesvd); -4 non-convergence or non-finite
+ * state; -5 output-file error; -6 CUDA error or no device; -7 bad argument.
+ */
+#ifndef EVP_B200_H
+#define EVP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct evp_solve evp_solve;
+
+/* Caller-owned summary of one solve. */
+typedef struct evp_report {
+    int status;                  /* final status code */
+    int macrosteps;              /* macrosteps completed */
+    long long equilibrium_iters; /* sum of global equilibrium iterations executed (the `iter` column) */
+    long long voxel_iters;       /* equilibrium_iters * number of voxels */
+    double wall_s;               /* host wall time of the solve, seconds */
+    double gpu_s;                /* device time of the macrostep loop (CUDA events), seconds */
+    int n1, n2, n3;              /* grid */
+} evp_report;
+
+/* Flags for evp_open. */
+#define EVP_WRITE_FILES 1  /* write results.csv, diagnostics.csv and VTK like the executable */
+#define EVP_VERBOSE 2      /* print the progress line (various_functions.f90:2693-2743) */
+
+/* Whole solve with the executable's semantics: replaces one
+ * `LS-EVPFFT --in fft_in --out out_dir --mix mix --modal modal` process
+ * (LS-EVPFFT.f90:87-595).  nthreads and fftw_save are accepted for the same
+ * command line and ignored (there is no FFTW planner). */
+int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const char* fftw_save, int mix, int modal,
+                   evp_report* report);
+
+/* Step-wise form of the same solve, for tests and the serving loop.
+ * evp_open = load_input + initial_guess + start-up c0 (LS-EVPFFT.f90:144-178);
+ * evp_advance runs up to nmacro macrosteps of LS-EVPFFT.f90:198-589 and
+ * reports how many ran in *done (0 once the deck is finished). */
+int evp_open(const char* fft_in, const char* out_dir, int mix, int modal, int flags, evp_solve** out);
+int evp_advance(evp_solve* s, int nmacro, int* done);
+
+/* Copy a per-voxel field to host memory (voxel v = i + n1*(j + n2*k),
+ * components innermost, 3x3 tensors row-major).  Names: sg, sgt, velgrad,
+ * velgradold, defgrad, defgradinv, defgrade, defgradp, edotp, ept,
+ * disgradsym, dvelgradref, gamdot, crss, trialtau, sch, c066mod, sg66, detF,
+ * wgtc, gacumgr, epvm, xnode.  *written = number of doubles copied. */
+int evp_get_field(evp_solve* s, const char* name, double* host_out, long long capacity, long long* written);
+
+/* Last results.csv row (53 values, IO_functions.f90:1264-1271 order) and
+ * diagnostics.csv row (44 values, types.f90:787-798 order). */
+int evp_last_rows(evp_solve* s, double* results53, double* diag44);
+int evp_stats(evp_solve* s, evp_report* out);
+int evp_close(evp_solve* s);
+
+/* Message of the last failing call on this thread. */
+const char* evp_last_error(void);
+int evp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
