@@ -311,7 +311,7 @@ __global__ void k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restri
                         for (int l = 0; l < 3; l++) x += c0[((i * 3 + jj) * 3 + k) * 3 + l] * (xi[jj] * xi[l]);
                     A[3 * i + k] = x;
                 }
-            if (inv3(A, ai) != 0) atomicOr(d.err, 1);
+            if (inv3u(A, ai) != 0) atomicOr(d.err, 1);
             // r_ij = -xi_j * sum_k ai_ik (P xi)_k
             double2 pv[3], wv[3];
 #pragma unroll

@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict
         }
         b6_to_s6(sg6, s6);
         st6(d.sg, N, v, s6);
-        if (lu_inverse(cg66, 6) != 0) set_err(d.err, 1);
+        if (inv_unrolled<6>(cg66) != 0) set_err(d.err, 1);
         for (int c = 0; c < 36; c++) d.sg66[c * N + v] = cg66[c];
         const double hps = hp[v];
         for (int s = 0; s < ph.nsyst; s++) {
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __rest
             ld9(d.Fe, N, v, Fe);
             ld9(d.ag, N, v, ag);
             mm3(Fe, ag, aa);
-            if (inv3(aa, ai) != 0) set_err(d.err, 1);
+            if (inv3u(aa, ai) != 0) set_err(d.err, 1);
             for (int s = 0; s < ph.nsyst; s++) {
                 double S[9], t[9], r[9], rs[9], b5[5];
                 for (int i = 0; i < 3; i++)
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kBlock) k_gas_compl(Dev d, double tdot, double
                 a[6 * i + j] = ((i == j) ? 1.0 : 0.0) + d.c066mod[(6 * i + j) * N + v] / tdot * complgas;
                 if (modal) a[6 * i + j] = a[6 * i + j] - d.cG[(6 * i + j) * N + v];
             }
-        if (lu_inverse(a, 6) != 0) set_err(d.err, 1);
+        if (inv_unrolled<6>(a) != 0) set_err(d.err, 1);
         for (int c = 0; c < 36; c++) d.cgas[c * N + v] = a[c];
     }
 }
@@ -711,7 +711,7 @@ __global__ void __launch_bounds__(kBlock) k_upd1(Dev d, Upd1Params p) {
         ld9(d.F, N, v, F);
         mm3(ex, F, F);
         const double detF = det33(F);
-        if (inv3(F, Fi) != 0) set_err(d.err, 1);
+        if (inv3u(F, Fi) != 0) set_err(d.err, 1);
         st9(d.F, N, v, F);
         st9(d.Finv, N, v, Fi);
         st9(d.Finc, N, v, ex);
@@ -753,9 +753,9 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
             const PhaseDev& ph = d.ph[d.phase[v]];
             double Fe[9], Feo[9], Fp[9], Fpi[9], F[9];
             ld9(d.Fe, N, v, Fe);
-            if (inv3(Fe, Feo) != 0) set_err(d.err, 1);
+            if (inv3u(Fe, Feo) != 0) set_err(d.err, 1);
             ld9(d.Fp, N, v, Fp);
-            if (inv3(Fp, Fpi) != 0) set_err(d.err, 1);
+            if (inv3u(Fp, Fpi) != 0) set_err(d.err, 1);
             ld9(d.F, N, v, F);
             mm3(F, Fpi, Fe);
             mm3(Fe, Feo, Feinc);
@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
             rotate4(aa, ph.C, c4);
             for (int c = 0; c < 81; c++) c4[c] = c4[c] / detFe;
             t4_to_b66(c4, c66);
-            if (lu_inverse(c66, 6) != 0) set_err(d.err, 1);
+            if (inv_unrolled<6>(c66) != 0) set_err(d.err, 1);
             for (int c = 0; c < 36; c++) d.sg66[c * N + v] = c66[c];
         } else {
             ld9(d.Feinc, N, v, Feinc);
@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
         // update_tensor_config pass 1 (various_functions.f90:2425-2466)
         const double detei = det33(Feinc);
         double Fii[9];
-        if (inv3(Finc, Fii) != 0) set_err(d.err, 1);
+        if (inv3u(Finc, Fii) != 0) set_err(d.err, 1);
         if (!gas) {
             double R[9], U[9], t[9], m[9], a6[6];
             polar(Finc, R, U);
@@ -839,7 +839,7 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
             va[f] = x;
             fc[f] = __ldcg(&d.red[OFF_UPD1 + 9 + f]) / dav;
         }
-        if (inv3(fc, di) != 0) set_err(d.err, 1);
+        if (inv3u(fc, di) != 0) set_err(d.err, 1);
         for (int f = 0; f < 9; f++) dd[f] = p.velgradavg[f] - va[f];
         mm3(dd, di, du);
         for (int f = 0; f < 9; f++) d.red[OFF_DU2 + f] = du[f];
@@ -1051,7 +1051,7 @@ __global__ void __launch_bounds__(kBlock) k_c0(Dev d, double tdot, double tdotre
         double tr[36];
         for (int i = 0; i < 6; i++)
             for (int j = 0; j < 6; j++) tr[6 * i + j] = d.sg66[(6 * i + j) * N + v] / tdot * tdot / tdotref + dd_at(dd, i, j);
-        if (lu_inverse(tr, 6) != 0) set_err(d.err, 1);
+        if (inv_unrolled<6>(tr) != 0) set_err(d.err, 1);
         double dsg[81], dpg[81], dp6[36], Fi[9];
         b66_to_t4(tr, dsg);
         ld9(d.Finv, N, v, Fi);
@@ -1172,7 +1172,7 @@ __global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restr
                     for (int l = 0; l < 3; l++) x += c0[((i * 3 + j) * 3 + k) * 3 + l] * (xi[j] * xi[l]);
                 A[3 * i + k] = x;
             }
-        if (inv3(A, a) != 0) set_err(d.err, 1);
+        if (inv3u(A, a) != 0) set_err(d.err, 1);
         for (int p = 0; p < 3; p++)
             for (int q = 0; q < 3; q++)
                 for (int i = 0; i < 3; i++)

@@ -235,6 +235,112 @@ EVP_HD int inv3(const double* a, double* ai) {
     return lu_inverse(ai, 3);
 }
 
+// Register-resident LU factorisation with partial pivoting (dgetrf pivot
+// choice), rows swapped in place; the permutation is not recorded (dgecon
+// does not use it).  Returns the dgetrf info value.
+template <int n>
+EVP_HD int lu_unrolled(double* J) {
+    int info = 0;
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double amax = fabs(J[k * n + k]);
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            double t = fabs(J[i * n + k]);
+            if (t > amax) { amax = t; p = i; }
+        }
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < n; j++) {
+                double x = J[k * n + j], y = J[i * n + j];
+                J[k * n + j] = sw ? y : x;
+                J[i * n + j] = sw ? x : y;
+            }
+        }
+        const double piv = J[k * n + k];
+        if (piv == 0.0 && info == 0) info = k + 1;
+        const double r = 1.0 / piv;
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const double l = J[i * n + k] * r;
+            J[i * n + k] = l;
+#pragma unroll
+            for (int j = k + 1; j < n; j++) J[i * n + j] -= l * J[k * n + j];
+        }
+    }
+    return info;
+}
+
+// Register-resident inverse of an n x n matrix (n = 3 or 6): LU with partial
+// pivoting (dgetrf pivot choice) applied to [A | I], then back substitution.
+// Every index is a compile-time constant, so nothing lives in addressable
+// local memory.  Returns the dgetrf info value.
+template <int n>
+EVP_HD int inv_unrolled(double* a) {
+    double J[n * n], B[n * n];
+#pragma unroll
+    for (int i = 0; i < n * n; i++) {
+        J[i] = a[i];
+        B[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
+    }
+    int info = 0;
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double amax = fabs(J[k * n + k]);
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            double t = fabs(J[i * n + k]);
+            if (t > amax) { amax = t; p = i; }
+        }
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < n; j++) {
+                double x = J[k * n + j], y = J[i * n + j];
+                J[k * n + j] = sw ? y : x;
+                J[i * n + j] = sw ? x : y;
+                double u = B[k * n + j], w = B[i * n + j];
+                B[k * n + j] = sw ? w : u;
+                B[i * n + j] = sw ? u : w;
+            }
+        }
+        const double piv = J[k * n + k];
+        if (piv == 0.0 && info == 0) info = k + 1;
+        const double r = 1.0 / piv;
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const double l = J[i * n + k] * r;
+#pragma unroll
+            for (int j = k + 1; j < n; j++) J[i * n + j] -= l * J[k * n + j];
+#pragma unroll
+            for (int j = 0; j < n; j++) B[i * n + j] -= l * B[k * n + j];
+        }
+    }
+#pragma unroll
+    for (int i = n - 1; i >= 0; i--) {
+#pragma unroll
+        for (int j = 0; j < n; j++) {
+            double s = B[i * n + j];
+#pragma unroll
+            for (int m = i + 1; m < n; m++) s -= J[i * n + m] * B[m * n + j];
+            B[i * n + j] = s / J[i * n + i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < n * n; i++) a[i] = B[i];
+    return info;
+}
+EVP_HD int inv3u(const double* a, double* ai) {
+#pragma unroll
+    for (int i = 0; i < 9; i++) ai[i] = a[i];
+    return inv_unrolled<3>(ai);
+}
+
 // Register-resident 6x6 solve J x = b with partial pivoting (dgesv), fully unrolled.
 EVP_HD int solve6(double (&J)[36], double (&b)[6]) {
     int info = 0;
@@ -322,16 +428,11 @@ EVP_HD int expm_adaptive(const double* a, double* e) {
     for (int i = 0; i < 9; i++) t1[i] = b12 * A6[i] + b10 * A4[i] + b8 * A2[i];
     mm3(A6, t1, V);
     for (int i = 0; i < 9; i++) V[i] = V[i] + b6 * A6[i] + b4 * A4[i] + b2 * A2[i] + b0 * ((i % 4 == 0) ? 1.0 : 0.0);
-    double Q[9];
-    int piv[3];
-    for (int i = 0; i < 9; i++) Q[i] = V[i] - U[i];
-    int info = lu_factor(Q, 3, piv);
+    double Q[9], P[9];
+    for (int i = 0; i < 9; i++) { Q[i] = V[i] - U[i]; P[i] = V[i] + U[i]; }
+    int info = inv_unrolled<3>(Q);
     if (info != 0) return info;
-    for (int c = 0; c < 3; c++) {
-        double col[3] = {V[c] + U[c], V[3 + c] + U[3 + c], V[6 + c] + U[6 + c]};
-        lu_solve(Q, 3, piv, col);
-        e[c] = col[0]; e[3 + c] = col[1]; e[6 + c] = col[2];
-    }
+    mm3(Q, P, e);
     for (int k = 0; k < s; k++) mm3(e, e, e);
     return 0;
 }
@@ -456,7 +557,6 @@ EVP_HD void stretch_rot(const double* Finc, bool cof_det, double& volinc, double
 EVP_HD double cond1_est_6x6(const double* Ain) {
     const int n = 6;
     double lu[36];
-    int piv[6];
     double anorm = 0.0;
     for (int j = 0; j < n; j++) {
         double cs = 0.0;
@@ -464,7 +564,7 @@ EVP_HD double cond1_est_6x6(const double* Ain) {
         anorm = fmax(anorm, cs);
     }
     for (int i = 0; i < 36; i++) lu[i] = Ain[i];
-    if (lu_factor(lu, n, piv) != 0) return EVP_HUGE;
+    if (lu_unrolled<6>(lu) != 0) return EVP_HUGE;
     double x[6], v[6];
     int isgn[6];
     auto solveA = [&](double* y) {

@@ -1028,6 +1028,14 @@ public:
         if (name == "sch") return soa_to_aos(d.sch, 5 * ns, m.data(), 5 * ns);
         if (name == "c066mod") return soa_to_aos(d.c066mod, 36, m.data(), 36);
         if (name == "sg66") return soa_to_aos(d.sg66, 36, m.data(), 36);
+        if (name == "macro") {  // c066, c0, s0, de_ds (reference-medium state, host copies)
+            if (cap < 279) return -1;
+            std::memcpy(out, c066, sizeof(c066));
+            std::memcpy(out + 36, c0, sizeof(c0));
+            std::memcpy(out + 117, s0, sizeof(s0));
+            std::memcpy(out + 198, de_ds, sizeof(de_ds));
+            return 279;
+        }
         if (name == "xnode") {
             long long n = 3LL * (d.n1 + 1) * (d.n2 + 1) * d.n3node;
             if (n > cap) return -1;

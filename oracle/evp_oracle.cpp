@@ -1925,6 +1925,14 @@ struct Oracle {
         if (name == "wgtc") return put1(&Voxel::wgtc);
         if (name == "gacumgr") return put1(&Voxel::gacumgr);
         if (name == "epvm") return put1(&Voxel::epvm);
+        if (name == "macro") {  // c066, c0, s0, de_ds (reference-medium state)
+            if (n < 279) return -1;
+            std::memcpy(out, c066, sizeof(M6));
+            std::memcpy(out + 36, c0, sizeof(T4));
+            std::memcpy(out + 117, s0, sizeof(T4));
+            std::memcpy(out + 198, de_ds, sizeof(T4));
+            return 279;
+        }
         if (name == "xnode") {
             long m = (long)xnode.size();
             if (m > n) return -1;
