@@ -1,0 +1,339 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the B200 LS-EVPFFT solve (plain FP64 path).
+
+Workload (one B200): large-strain strain-rate-controlled tension, 64^3 voxels,
+500 periodic-Voronoi grains (seed 2), FCC power law n=20, udot33=1e-3/s,
+dt=0.5 s increments with lattice rotation and grid update (iupdate=1).
+Synthetic seeded inputs in the reference's file grammar stand in for the
+reference's (unshipped) microstructures.  A "step" is one macrostep
+(increment): every equilibrium iteration it needs plus the large-strain
+updates.  Metric: voxel-iters/s = voxels x equilibrium iterations / device
+seconds (CUDA events on the solver's stream, max over ranks).  The state
+(~1.8 kB/voxel, 460 MB) is larger than the 126 MB L2, so no flush is needed.
+
+--gpus N > 1 runs N independent replicas (the solve does not shard), one
+process per GPU, and sums their voxel-iters.
+--impl reference times the CPU oracle (a C++ restatement of the reference
+Fortran/OpenMP solver; the Fortran build itself cannot be compiled here) on
+the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "voxel-iters/s"
+# Algorithmic HBM bytes per voxel and launch of the equilibrium-iteration kernels
+# (FP64 state, 12 slip systems; spectrum terms scale with (n1/2+1)/n1).
+def algorithmic_bytes(n1: int, nsys: int = 12) -> dict:
+    half = (n1 // 2 + 1) / n1
+    spec = 9 * 16 * half  # one pass over the 9-component half spectrum, per voxel
+    return {
+        "k_sgavg": 7 * 8,
+        "k_fft_x_fwd": 16 * 8 + spec,
+        "k_fft_y_fwd": 2 * spec,
+        "k_fft_z_green": 2 * spec,
+        "k_fft_y_inv": 2 * spec,
+        "k_fft_x_inv": spec + (9 + 1 + 9) * 8,
+        "k_corr": (9 * 4 + 1) * 8 + 1 + 9 * 2 * 8,
+        # velgrad 9, sg 6, sgt 6, wgtc 1, trialtau 2n, gacumgr 1, crss 2n, sch 5n, C~ 36, S 36 | sg 6, edotp 6, gamdot n, trialtau 2n
+        "k_newton": (9 + 6 + 6 + 1 + 2 * nsys + 1 + 2 * nsys + 5 * nsys + 36 + 36 + 6 + 6 + nsys + 2 * nsys) * 8 + 2,
+    }
+
+
+LAUNCHES_PER_RECORD = {"k_grid_fft": 5}
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or not f[0].isdigit() or int(f[0]) != self.index:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_deck(root: Path, n: int, nsteps: int, ngrains: int) -> Path:
+    from creep_modeling_b200 import decks
+
+    case = decks.case_c2(nsteps=nsteps, n=n, ngrains=ngrains)
+    return decks.write_case(case, root)
+
+
+def cpu_baseline(fft: Path, nmacro: int, budget_s: float) -> dict:
+    """The oracle on all host cores, on a bounded sample of the same workload."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    s = oracle.OracleSolve(fft, mix=1, modal=0, nthreads=threads)
+    done = iters0 = 0
+    iters0 = s.total_iters()
+    t0 = time.perf_counter()
+    while done < nmacro:
+        if s.advance(1) != 1:
+            break
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    vi = (s.total_iters() - iters0) * s.nvox
+    s.close()
+    return {"value": vi / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"first {done} increment(s) of the same {s.shape[0]}^3 tension deck ({vi} voxel-iters, {dt:.1f} s)"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    n = args.n
+    with tempfile.TemporaryDirectory() as td:
+        fft = make_deck(Path(td), n, args.warmup + args.steps + 1, args.ngrains)
+        import oracle
+
+        threads = os.cpu_count() or 1
+        s = oracle.OracleSolve(fft, mix=1, modal=0, nthreads=threads)
+        budget = args.ref_budget
+        t_all = time.perf_counter()
+        wdone = 0
+        for _ in range(args.warmup):
+            if time.perf_counter() - t_all > budget / 3:
+                break
+            s.advance(1)
+            wdone += 1
+        it0 = s.total_iters()
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(args.steps):
+            s.advance(1)
+            done += 1
+            if time.perf_counter() - t_all > budget:
+                break
+        dt = time.perf_counter() - t0
+        vi = (s.total_iters() - it0) * s.nvox
+        value = vi / dt
+        sample = (f"{done} timed increment(s) after {wdone} warm-up of the {n}^3 tension deck on {threads} host threads "
+                  f"(C++ FP64 restatement of the reference Fortran solver)")
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": done,
+                "warmup": wdone, "ms_per_step": dt / max(done, 1) * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"tension {n}^3, 500 grains, n=20, udot33=1e-3/s, dt=0.5 s, iupdate=1",
+                           "voxels": n ** 3, "l2": "state larger than L2"},
+                "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="grid edge (default: the 64^3 configuration)")
+    ap.add_argument("--ngrains", type=int, default=500)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds of CPU time for --impl reference")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    import torch
+
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    else:
+        torch.cuda.set_device(0)
+    from creep_modeling_b200 import Solve
+
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    n = args.n
+    td = tempfile.mkdtemp(prefix=f"evp_bench_r{rank}_")
+    fft = make_deck(Path(td), n, args.warmup + args.steps + 1, args.ngrains)
+    s = Solve(fft, mix=1, modal=0, profile=True)
+    for _ in range(args.warmup):
+        s.advance(1)
+    clocks = ClockSampler(local if ws > 1 else 0)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    st0 = s.stats()
+    kt0 = s.kernel_times()
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.advance(1)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    if pg:
+        pg.barrier()
+    st1 = s.stats()
+    kt1 = s.kernel_times()
+    gpu_s = st1.gpu_s - st0.gpu_s
+    vi = (st1.equilibrium_iters - st0.equilibrium_iters) * s.nvox
+    iters = st1.equilibrium_iters - st0.equilibrium_iters
+    if pg:
+        t = torch.tensor([gpu_s, float(vi)], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
+        pg.all_reduce(t, op=pg.ReduceOp.SUM)
+        gpu_s_max, vi_tot = float(tmax[0]), float(t[1])
+    else:
+        gpu_s_max, vi_tot = gpu_s, float(vi)
+    value = vi_tot / gpu_s_max
+    # per-kernel device time in the timed region
+    kd = {}
+    launches = 0
+    for k, (cnt, ms) in kt1.items():
+        c0, m0 = kt0.get(k, (0, 0.0))
+        kd[k] = (cnt - c0, ms - m0)
+        launches += (cnt - c0) * LAUNCHES_PER_RECORD.get(k, 1)
+    s.close()
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel
+    peak, peak_kind = load_peaks()
+    ab = algorithmic_bytes(n)
+    dom = max(kd, key=lambda k: kd[k][1]) if kd else None
+    roof = None
+    if dom:
+        cnt, ms = kd[dom]
+        avg_s = ms / 1e3 / max(cnt, 1)
+        bytes_launch = ab.get(dom, 0.0) * n ** 3
+        ach = bytes_launch / avg_s / 1e9 if bytes_launch else None
+        traffic = None
+        tp = ROOT / "profiles" / f"{dom}_traffic.json"
+        if tp.exists():
+            try:
+                traffic = json.loads(tp.read_text()).get("bytes_per_launch_scaled")
+            except Exception:
+                traffic = None
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": (ach / peak if ach else None), "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                "avg_launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": bytes_launch,
+                "kernel_share": {k: round(v[1] / max(sum(x[1] for x in kd.values()), 1e-30), 4) for k, v in
+                                 sorted(kd.items(), key=lambda kv: -kv[1][1])}}
+
+    # end to end through the C ABI with host buffers: deck files -> device -> CSV rows
+    e2e = None
+    try:
+        with tempfile.TemporaryDirectory() as td2:
+            fft2 = make_deck(Path(td2), n, args.steps + 1, args.ngrains)
+            out = Path(td2) / "out"
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            s2 = Solve(fft2, out_dir=out, mix=1, modal=0, csv_only=True)
+            for _ in range(args.steps):
+                s2.advance(1)
+            r2 = s2.stats()
+            s2.close()
+            torch.cuda.synchronize(dev)
+            we = time.perf_counter() - t0
+            e2e = {"value": r2.voxel_iters / we, "unit": METRIC,
+                   "h2d_bytes_per_step": int(r2.h2d_bytes / max(args.steps, 1)),
+                   "d2h_bytes_per_step": int(r2.d2h_bytes / max(args.steps, 1)),
+                   "note": "evp_open (deck files parsed and uploaded) + steps + results/diagnostics CSV rows, host wall clock"}
+    except Exception as exc:  # pragma: no cover - reported, not hidden
+        e2e = {"value": None, "unit": METRIC, "error": str(exc)}
+
+    cpu = None
+    if not args.no_cpu:
+        try:
+            cpu = cpu_baseline(fft, args.cpu_steps, 60.0)
+        except Exception as exc:  # pragma: no cover
+            cpu = {"value": None, "error": str(exc)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": gpu_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"tension {n}^3, {args.ngrains} grains, n=20, udot33=1e-3/s, dt=0.5 s, iupdate=1 "
+                               "(plain FP64)", "voxels": n ** 3, "equilibrium_iters": int(iters),
+                   "parallelism": f"replicas x{ws}", "l2": "state (~460 MB) larger than L2; no flush"},
+        "wall_s": wall, "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+    }
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

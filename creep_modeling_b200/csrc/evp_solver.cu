@@ -138,18 +138,70 @@ public:
         if (st) cudaStreamDestroy(st);
     }
 
+    // ---- host<->device byte counters and the optional per-kernel event timer
+    long long h2d = 0, d2h = 0;
+    bool profile = false, write_vtk_files = false;
+    struct KTime {
+        std::string name;
+        long long n = 0;
+        double ms = 0.0;
+    };
+    std::vector<KTime> ktimes;
+    struct Pending {
+        int k;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pend;
+    std::vector<cudaEvent_t> evpool;
+    cudaEvent_t get_ev() {
+        if (!evpool.empty()) { cudaEvent_t e = evpool.back(); evpool.pop_back(); return e; }
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    template <class F>
+    void K(const char* name, F&& f) {
+        if (!profile) { f(); return; }
+        int k = -1;
+        for (size_t i = 0; i < ktimes.size(); i++)
+            if (ktimes[i].name == name) { k = (int)i; break; }
+        if (k < 0) { ktimes.push_back(KTime{name}); k = (int)ktimes.size() - 1; }
+        cudaEvent_t a = get_ev(), b = get_ev();
+        CK(cudaEventRecord(a, st));
+        f();
+        CK(cudaEventRecord(b, st));
+        pend.push_back(Pending{k, a, b});
+    }
+    void resolve_timers() {
+        for (auto& p : pend) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) { ktimes[p.k].n++; ktimes[p.k].ms += ms; }
+            evpool.push_back(p.a);
+            evpool.push_back(p.b);
+        }
+        pend.clear();
+    }
+    void h2d_copy(void* dst, const void* src, size_t bytes) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        h2d += (long long)bytes;
+    }
+
     void sync() { CK(cudaStreamSynchronize(st)); }
     void fetch_red() {
         CK(cudaMemcpyAsync(h_red, d.red, RED_OUT_SIZE * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(h_err, d.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        d2h += RED_OUT_SIZE * sizeof(double) + sizeof(int);
         sync();
+        resolve_timers();
         if (*h_err & 1) throw SolveError("singular matrix in a voxel operator (lu_inverse / lu_eqsystem)", -3);
         if (*h_err & 2) throw SolveError("non-finite stress in the local Newton solve", -4);
     }
 
     // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
     void open(const std::string& fft_in, const std::string& out, int mix_flag, int modal_flag, int flags) {
-        write_files = (flags & EVP_WRITE_FILES) != 0;
+        write_files = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) != 0;
+        write_vtk_files = (flags & EVP_WRITE_FILES) != 0;
+        profile = (flags & EVP_PROFILE) != 0;
         verbose = (flags & EVP_VERBOSE) != 0;
         outdir = out.empty() ? std::string("evpfft_outputs/") : out;
         if (write_files) {
@@ -180,7 +232,7 @@ public:
         const ProcessData& p1 = dk.process[0];
         dvmavg = vm_strain(p1.dsim);
         lvmavg = dvmavg;
-        if (write_files) write_vtk(0);
+        if (write_vtk_files) write_vtk(0);
         // start-up tangent (LS-EVPFFT.f90:156-173)
         for (int c = 0; c < 36; c++) c066[c] = h_red[OFF_INIT + c] / wphcsol * p1.tdot;
         for (int c = 0; c < 36; c++) s066[c] = c066[c];
@@ -247,7 +299,7 @@ public:
                 long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)n;
                 t[e] = make_double2((double)cosl(ang), (double)sinl(ang));
             }
-            CK(cudaMemcpyAsync(dst, t.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+            h2d_copy(dst, t.data(), n * sizeof(double2));
             sync();
         };
         twiddles(dk.n1, d.tw1); twiddles(dk.n2, d.tw2); twiddles(dk.n3, d.tw3);
@@ -280,7 +332,7 @@ public:
             for (int c = 0; c < 81; c++) t.C[c] = s.C[c];
         }
         PhaseDev* dph = dalloc<PhaseDev>(dk.nph);
-        CK(cudaMemcpyAsync(dph, ph.data(), dk.nph * sizeof(PhaseDev), cudaMemcpyHostToDevice, st));
+        h2d_copy(dph, ph.data(), dk.nph * sizeof(PhaseDev));
         d.ph = dph;
         d.nph = dk.nph;
     }
@@ -300,16 +352,16 @@ public:
         for (int c = 0; c < 9; c++) {
             defgradavg[c] = dinvc[c] = dinvcs[c] = dinvcg[c] = (c % 4 == 0) ? 1.0 : 0.0;
         }
-        CK(cudaMemcpyAsync(d.gas, gas.data(), N, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.phase, phs.data(), N, cudaMemcpyHostToDevice, st));
-        if (d.eth) CK(cudaMemcpyAsync(d.eth, dk.eth.data(), 9 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+        h2d_copy(d.gas, gas.data(), N);
+        h2d_copy(d.phase, phs.data(), N);
+        if (d.eth) h2d_copy(d.eth, dk.eth.data(), 9 * N * sizeof(double));
         for (auto& p : dk.process) has_thermo = has_thermo || p.ithermo == 1;
         double* d_eul = dalloc<double>(3 * N);
         int* d_gr = dalloc<int>(N);
         double* d_hp = dalloc<double>(N);
-        CK(cudaMemcpyAsync(d_eul, dk.euler.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_gr, dk.grain.data(), N * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_hp, dk.hp_shift.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+        h2d_copy(d_eul, dk.euler.data(), 3 * N * sizeof(double));
+        h2d_copy(d_gr, dk.grain.data(), N * sizeof(int));
+        h2d_copy(d_hp, dk.hp_shift.data(), N * sizeof(double));
         // xnode start values (types.f90:273-287)
         {
             const int n1 = dk.n1, n2 = dk.n2, nn3 = d.n3node;
@@ -322,7 +374,7 @@ public:
                         xn[p + 1] = (double)(j + 1) - 0.5;
                         xn[p + 2] = (nn3 == 1) ? 0.0 : (double)(k + 1) - 0.5;
                     }
-            CK(cudaMemcpyAsync(d.xnode, xn.data(), xn.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            h2d_copy(d.xnode, xn.data(), xn.size() * sizeof(double));
         }
         const ProcessData& p1 = dk.process[0];
         double u6[6], u6t[6];
@@ -339,8 +391,8 @@ public:
     }
 
     void upload_c0() {
-        CK(cudaMemcpyAsync(d_c0, c0, sizeof(c0), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_s0, s0, sizeof(s0), cudaMemcpyHostToDevice, st));
+        h2d_copy(d_c0, c0, sizeof(c0));
+        h2d_copy(d_s0, s0, sizeof(s0));
     }
 
     // ------------------------------------------------------------ snapshots (various_functions.f90:2839-2895)
@@ -450,21 +502,21 @@ public:
     // ------------------------------------------------------------ one equilibrium iteration (LS-EVPFFT.f90:233-359)
     void equilibrium_iteration(bool fresh_sgavg) {
         ProcessData& p = P();
-        if (fresh_sgavg) launch_sgavg(d, st);
-        launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st);
-        launch_fft_y(d, pl2, 9, false, st);
-        launch_fft_z_green(d, pl3, d_c0, d_s0, st);
-        launch_fft_y(d, pl2, 9, true, st);
+        if (fresh_sgavg) K("k_sgavg", [&] { launch_sgavg(d, st); });
+        K("k_fft_x_fwd", [&] { launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st); });
+        K("k_fft_y_fwd", [&] { launch_fft_y(d, pl2, 9, false, st); });
+        K("k_fft_z_green", [&] { launch_fft_z_green(d, pl3, d_c0, d_s0, st); });
+        K("k_fft_y_inv", [&] { launch_fft_y(d, pl2, 9, true, st); });
         XinvParams xp;
         std::memcpy(xp.dvelgradavg, dvelgradavg, sizeof(xp.dvelgradavg));
         if (inv3(dinvc, xp.dinv) != 0) throw SolveError("Singular matrix in lu_inverse (correction_to_current)", -3);
-        launch_fft_x_inv(d, pl1, 0, xp, st);
+        K("k_fft_x_inv", [&] { launch_fft_x_inv(d, pl1, 0, xp, st); });
         CorrParams cp;
         cp.mix = mix;
         cp.Lscale = std::max(lvmavg, EVP_TINY);
         cp.do_mix = do_mix ? 1 : 0;
         cp.kinematic = kinematic ? 1 : 0;
-        launch_corr(d, cp, st);
+        K("k_corr", [&] { launch_corr(d, cp, st); });
         NewtonParams np;
         np.tdot = p.tdot;
         np.error = p.error;
@@ -473,7 +525,7 @@ public:
         np.modal = modal ? 1 : 0;
         np.thermo = (imicro == 1 && p.ithermo == 1) ? 1 : 0;
         np.iuphard = p.iuphard;
-        launch_newton(d, np, st);
+        K("k_newton", [&] { launch_newton(d, np, st); });
         CK(cudaGetLastError());
         fetch_red();
         const double* cr = h_red + OFF_CORR;
@@ -504,7 +556,7 @@ public:
     }
 
     int kinematic_substep(double tdot_step, double& min_detF) {
-        launch_kinematic(d, tdot_step, st);
+        K("k_kinematic", [&] { launch_kinematic(d, tdot_step, st); });
         CK(cudaGetLastError());
         fetch_red();
         const double mv = h_red[OFF_KIN], mr = h_red[OFF_KIN + 1], ms = h_red[OFF_KIN + 2];
@@ -536,17 +588,17 @@ public:
         bool did_converge = false, accept_step = false;
         const int do_schmid = ((imicro == 1 && ipr == 1) || p.iupdate == 1) ? 1 : 0;
         if (modal) {  // form_G: only the real-space origin value is needed (Gamma is applied on the fly)
-            launch_goperr0(d, d_c0, d_s0, st);
+            K("k_goperr0", [&] { launch_goperr0(d, d_c0, d_s0, st); });
             fetch_red();
             for (int c = 0; c < 81; c++) goperr0[c] = h_red[OFF_G0 + c] / (double)d.N;
-            CK(cudaMemcpyAsync(d_g0, goperr0, sizeof(goperr0), cudaMemcpyHostToDevice, st));
+            h2d_copy(d_g0, goperr0, sizeof(goperr0));
         }
-        launch_prologue(d, d_c0, d_g0, do_schmid, modal ? 1 : 0, st);
+        K("k_prologue", [&] { launch_prologue(d, d_c0, d_g0, do_schmid, modal ? 1 : 0, st); });
         iter = 0;
         bool fresh = true;
         while (!(did_converge || accept_step)) {
             if (iter == 0) {
-                if (dk.has_gas) launch_gas_compl(d, p.tdot, dk.complgas, modal ? 1 : 0, st);
+                if (dk.has_gas) K("k_gas_compl", [&] { launch_gas_compl(d, p.tdot, dk.complgas, modal ? 1 : 0, st); });
                 std::memset(dvelgradavg, 0, sizeof(dvelgradavg));
                 edotvmmx = 0;
                 mix = 1.0;
@@ -618,29 +670,31 @@ public:
         const int iter_done = iter;
         // commit + large-strain updates (LS-EVPFFT.f90:432-458)
         if (p.iupdate == 1) {  // update_grid_velgrad_node reads L and F before update_defgrad changes F
-            launch_fft_x_fwd(d, pl1, 1, 0, st);
-            launch_fft_y(d, pl2, 9, false, st);
-            launch_fft_z_integ(d, pl3, p.igamma, st);
-            launch_fft_y(d, pl2, 3, true, st);
-            XinvParams xp{};
-            launch_fft_x_inv(d, pl1, 1, xp, st);
-            launch_cell2node(d, p.tdot, p.igamma, st);
+            K("k_grid_fft", [&] {
+                launch_fft_x_fwd(d, pl1, 1, 0, st);
+                launch_fft_y(d, pl2, 9, false, st);
+                launch_fft_z_integ(d, pl3, p.igamma, st);
+                launch_fft_y(d, pl2, 3, true, st);
+                XinvParams xp{};
+                launch_fft_x_inv(d, pl1, 1, xp, st);
+            });
+            K("k_cell2node", [&] { launch_cell2node(d, p.tdot, p.igamma, st); });
         }
         Upd1Params u1;
         u1.tdot = p.tdot;
         u1.iupdate = p.iupdate;
-        launch_upd1(d, u1, st);
+        K("k_upd1", [&] { launch_upd1(d, u1, st); });
         if (p.iupdate == 1) {
             Upd2Params u2;
             std::memcpy(u2.velgradavg, velgradavg, sizeof(u2.velgradavg));
-            launch_upd2(d, u2, st);
+            K("k_upd2", [&] { launch_upd2(d, u2, st); });
         }
         Upd3Params u3;
         u3.tdot = p.tdot;
         u3.iupdate = p.iupdate;
         u3.iuphard = p.iuphard;
         u3.vlast = vlast;
-        launch_upd3(d, u3, st);
+        K("k_upd3", [&] { launch_upd3(d, u3, st); });
         // averages that only depend on host values
         double vsym[9];
         sym33(velgradavg, vsym);
@@ -648,7 +702,7 @@ public:
         dvmavg = vm_strain(vsym);
         evmavg = evmavg + dvmavg * p.tdot;
         const double Lref = std::max(lvmavg, EVP_TINY);
-        launch_diag(d, std::max(1.0e-12 * Lref, EVP_TINY), st);
+        K("k_diag", [&] { launch_diag(d, std::max(1.0e-12 * Lref, EVP_TINY), st); });
         // time bookkeeping and the tdot ramp are host-only; they fix the tdot calc_c0 sees
         const double tdot_used = p.tdot;
         const double tdotref_used = p.tdotref;
@@ -678,7 +732,7 @@ public:
             p.nsteps = imicro + left;
         }
         const bool conv_for_count = did_converge;
-        launch_c0(d, p.tdot, p.tdotref, st);
+        K("k_c0", [&] { launch_c0(d, p.tdot, p.tdotref, st); });
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev1, st));
         fetch_red();
@@ -717,7 +771,7 @@ public:
         if (p.iwfields == 1) {
             const int aw = std::abs(p.iwstep);
             const bool due = (aw != 0 && imicro % aw == 0) || (p.iwstep < 0 && imicro == p.nsteps);
-            if (due && write_files) write_vtk(imacroloop);
+            if (due && write_vtk_files) write_vtk(imacroloop);
         }
         finish_diag();
         dg.erre = erre; dg.errs = errs; dg.errsbc = errsbc;
@@ -848,6 +902,7 @@ public:
     std::vector<double> field_host(double* dp, size_t n) {
         std::vector<double> h(n);
         CK(cudaMemcpyAsync(h.data(), dp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        d2h += (long long)(n * sizeof(double));
         sync();
         return h;
     }
@@ -1132,7 +1187,26 @@ int evp_stats(evp_solve* h, evp_report* r) {
     r->wall_s = 0.0;
     r->gpu_s = h->s.gpu_ms * 1e-3;
     r->n1 = h->s.d.n1; r->n2 = h->s.d.n2; r->n3 = h->s.d.n3;
+    r->h2d_bytes = h->s.h2d;
+    r->d2h_bytes = h->s.d2h;
     return 0;
+}
+
+int evp_kernel_times(evp_solve* h, char* names, long long* launches, double* ms, int cap) {
+    if (!h) return fail("evp_kernel_times: null handle", -7);
+    const auto& kt = h->s.ktimes;
+    int n = 0;
+    for (const auto& k : kt) {
+        if (n >= cap) break;
+        if (names) {
+            std::strncpy(names + 32 * n, k.name.c_str(), 31);
+            names[32 * n + 31] = '\0';
+        }
+        if (launches) launches[n] = k.n;
+        if (ms) ms[n] = k.ms;
+        n++;
+    }
+    return n;
 }
 
 int evp_close(evp_solve* h) {

@@ -29,6 +29,8 @@ DIAG_COLS = (
 
 WRITE_FILES = 1
 VERBOSE = 2
+WRITE_CSV = 4
+PROFILE = 8
 
 
 def run_solver(fft_in, out_dir="evpfft_outputs/", nthreads=0, fftw_save="", mix=1, modal=1) -> _lib.Report:
@@ -46,10 +48,12 @@ def run_solver(fft_in, out_dir="evpfft_outputs/", nthreads=0, fftw_save="", mix=
 class Solve:
     """A device-resident solve advanced macrostep by macrostep."""
 
-    def __init__(self, fft_in, out_dir="", mix=1, modal=1, write_files=False, verbose=False):
+    def __init__(self, fft_in, out_dir="", mix=1, modal=1, write_files=False, verbose=False, csv_only=False,
+                 profile=False):
         L = _lib.load()
         h = ctypes.c_void_p()
-        flags = (WRITE_FILES if write_files else 0) | (VERBOSE if verbose else 0)
+        flags = ((WRITE_FILES if write_files else 0) | (VERBOSE if verbose else 0) | (WRITE_CSV if csv_only else 0)
+                 | (PROFILE if profile else 0))
         _lib.check(L.evp_open(str(fft_in).encode(), str(out_dir).encode(), int(mix), int(modal), flags, ctypes.byref(h)))
         self._h = h
         rep = self.stats()
@@ -81,6 +85,19 @@ class Solve:
         _lib.check(_lib.load().evp_get_field(self._h, name.encode(), buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap,
                                              ctypes.byref(n)))
         return buf[: n.value].copy()
+
+    def kernel_times(self) -> dict:
+        """{kernel: (launches, total ms)} recorded under ``profile=True``."""
+        cap = 64
+        names = ctypes.create_string_buffer(32 * cap)
+        launches = (ctypes.c_longlong * cap)()
+        ms = (ctypes.c_double * cap)()
+        n = _lib.load().evp_kernel_times(self._h, names, launches, ms, cap)
+        out = {}
+        for i in range(max(n, 0)):
+            nm = names.raw[32 * i: 32 * i + 32].split(b"\0", 1)[0].decode()
+            out[nm] = (int(launches[i]), float(ms[i]))
+        return out
 
     def stats(self) -> _lib.Report:
         rep = _lib.Report()

@@ -33,11 +33,15 @@ typedef struct evp_report {
     double wall_s;               /* host wall time of the solve, seconds */
     double gpu_s;                /* device time of the macrostep loop (CUDA events), seconds */
     int n1, n2, n3;              /* grid */
+    long long h2d_bytes;         /* host-to-device bytes copied so far (deck upload, per-step constants) */
+    long long d2h_bytes;         /* device-to-host bytes copied so far (per-iteration sums, fields) */
 } evp_report;
 
 /* Flags for evp_open. */
 #define EVP_WRITE_FILES 1  /* write results.csv, diagnostics.csv and VTK like the executable */
 #define EVP_VERBOSE 2      /* print the progress line (various_functions.f90:2693-2743) */
+#define EVP_WRITE_CSV 4    /* write results.csv and diagnostics.csv only (no VTK) */
+#define EVP_PROFILE 8      /* time every kernel launch with CUDA events (evp_kernel_times) */
 
 /* Whole solve with the executable's semantics: replaces one
  * `LS-EVPFFT --in fft_in --out out_dir --mix mix --modal modal` process
@@ -65,6 +69,11 @@ int evp_get_field(evp_solve* s, const char* name, double* host_out, long long ca
 int evp_last_rows(evp_solve* s, double* results53, double* diag44);
 int evp_stats(evp_solve* s, evp_report* out);
 int evp_close(evp_solve* s);
+
+/* Per-kernel device time under EVP_PROFILE: fills up to cap entries of
+ * names (each a NUL-terminated string of at most 31 chars, stored in
+ * names[32*i]), launches and milliseconds; returns the number of kernels. */
+int evp_kernel_times(evp_solve* s, char* names, long long* launches, double* ms, int cap);
 
 /* Message of the last failing call on this thread. */
 const char* evp_last_error(void);
