@@ -497,8 +497,87 @@ __global__ void k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, Xin
     }
 }
 
+// ---------------------------------------------------------------- standalone Green-operator application
+// x passes of evp_green_apply: the 9 real input fields come straight from a
+// caller-owned array tau[c*N + v] and the result goes to out[c*N + v].
+__global__ void k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restrict__ tau) {
+    extern __shared__ double2 s[];
+    const int n1 = d.n1, n1h = d.n1h;
+    const long long N = d.N;
+    const int nrows = d.n2 * d.n3;
+    const int P = 9 * G;
+    const int pair0 = blockIdx.x * G;
+    double* sd = reinterpret_cast<double*>(s);
+    for (int idx = threadIdx.x; idx < G * 2 * n1; idx += blockDim.x) {
+        const int g = idx / (2 * n1), rem = idx % (2 * n1), half = rem / n1, x = rem % n1;
+        const int row = 2 * (pair0 + g) + half;
+        const long long v = (long long)row * n1 + x;
+#pragma unroll
+        for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = (row < nrows) ? tau[c * N + v] : 0.0;
+    }
+    __syncthreads();
+    fft_run<false>(s, P, P, pl, d.tw1);
+    for (int idx = threadIdx.x; idx < P * n1h; idx += blockDim.x) {
+        const int k = idx % n1h, p = idx / n1h;
+        const int c = p / G, g = p % G;
+        const double2 Z = s[k * P + p];
+        const double2 Zc = cconj(s[((n1 - k) % n1) * P + p]);
+        const double2 dZ = csub(Z, Zc);
+        const int ra = 2 * (pair0 + g);
+        if (ra < nrows) d.spec[((long long)c * nrows + ra) * n1h + k] = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+        if (ra + 1 < nrows) d.spec[((long long)c * nrows + ra + 1) * n1h + k] = make_double2(0.5 * dZ.y, -0.5 * dZ.x);
+    }
+}
+__global__ void k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ out) {
+    extern __shared__ double2 s[];
+    const int n1 = d.n1, n1h = d.n1h;
+    const long long N = d.N;
+    const int nrows = d.n2 * d.n3;
+    const int P = 9 * G;
+    const int pair0 = blockIdx.x * G;
+    const bool even = (n1 % 2 == 0);
+    for (int idx = threadIdx.x; idx < P * n1; idx += blockDim.x) {
+        const int x = idx % n1, p = idx / n1;
+        const int c = p / G, g = p % G;
+        const int ra = 2 * (pair0 + g);
+        const int k = (x <= n1 / 2) ? x : n1 - x;
+        double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+        if (ra < nrows) A = d.spec[((long long)c * nrows + ra) * n1h + k];
+        if (ra + 1 < nrows) B = d.spec[((long long)c * nrows + ra + 1) * n1h + k];
+        if (k == 0 || (even && k == n1 / 2)) { A.y = 0.0; B.y = 0.0; }
+        if (x > n1 / 2) { A.y = -A.y; B.y = -B.y; }
+        s[x * P + p] = make_double2(A.x - B.y, A.y + B.x);
+    }
+    __syncthreads();
+    fft_run<true>(s, P, P, pl, d.tw1);
+    const double* sd = reinterpret_cast<const double*>(s);
+    for (int idx = threadIdx.x; idx < G * 2 * n1; idx += blockDim.x) {
+        const int g = idx / (2 * n1), rem = idx % (2 * n1), half = rem / n1, x = rem % n1;
+        const int row = 2 * (pair0 + g) + half;
+        if (row >= nrows) continue;
+        const long long v = (long long)row * n1 + x;
+#pragma unroll
+        for (int c = 0; c < 9; c++) out[c * N + v] = sd[2 * (x * P + c * G + g) + half] / (double)N;
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static int x_rows_per_block(int n1) { return (256 / n1) > 1 ? 256 / n1 : 1; }
+
+void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
+                        double* out, const double* c0, const double* s0, cudaStream_t st) {
+    const int G = x_rows_per_block(d.n1);
+    const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
+    const int grid = (npairs + G - 1) / G;
+    const int P = 9 * G;
+    const int thr = pick_threads(P, pl1, 256);
+    const size_t smem = (size_t)P * d.n1 * sizeof(double2);
+    k_green_x_fwd<<<grid, thr, smem, st>>>(d, pl1, G, tau);
+    launch_fft_y(d, pl2, 9, false, st);
+    launch_fft_z_green(d, pl3, c0, s0, st);
+    launch_fft_y(d, pl2, 9, true, st);
+    k_green_x_inv<<<grid, thr, smem, st>>>(d, pl1, G, out);
+}
 
 void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
     const int G = x_rows_per_block(d.n1);
@@ -564,6 +643,8 @@ void fft_configure() {
     cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     cudaFuncSetAttribute(k_fft_z_integ, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     cudaFuncSetAttribute(k_fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_green_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_green_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
 }
 
 }  // namespace evp

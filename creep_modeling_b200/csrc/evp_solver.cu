@@ -25,6 +25,7 @@
 namespace evp {
 
 static thread_local std::string g_last_error;
+void set_last_error(const std::string& m) { g_last_error = m; }
 
 struct SolveError : std::runtime_error {
     int code;

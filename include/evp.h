@@ -75,6 +75,18 @@ int evp_close(evp_solve* s);
  * names[32*i]), launches and milliseconds; returns the number of kernels. */
 int evp_kernel_times(evp_solve* s, char* names, long long* launches, double* ms, int cap);
 
+/* Operator-level entry: applies the periodic Green operator of a homogeneous
+ * reference medium to a polarization field, the inner operator of every
+ * equilibrium iteration (convolution_with_Goper with form_G igamma = 0,
+ * lsevpfft/src/various_functions.f90:640-809 and 966-1059).
+ * d_tau, d_out: caller-owned device arrays of 9 x N doubles, component c = 3*i+j
+ * outermost (field[c*N + v], v = i + n1*(j + n2*k)); d_out may not alias d_tau.
+ * c0, s0: host arrays of 81 doubles, the reference stiffness and its
+ * compliance (4th-order, index ((i*3+j)*3+k)*3+l).  stream: a cudaStream_t or
+ * NULL.  The scratch spectrum is allocated and freed inside the call. */
+int evp_green_apply(const double* d_tau, double* d_out, int n1, int n2, int n3, const double* c0, const double* s0,
+                    void* stream);
+
 /* Message of the last failing call on this thread. */
 const char* evp_last_error(void);
 int evp_version(void);

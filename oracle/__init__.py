@@ -65,6 +65,8 @@ def lib():
         L.oracle_cond1_6x6.restype = ctypes.c_double
         L.oracle_fft3.argtypes = [c_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_plastic_rate.argtypes = [c_dp, c_dp, c_dp, c_dp, ctypes.c_int, c_dp, c_dp, c_dp, c_dp]
+        L.oracle_green_apply.argtypes = [c_dp, c_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp]
+        L.oracle_green_apply.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -181,6 +183,19 @@ def polar(f):
 def cond1(a66):
     a = np.ascontiguousarray(a66, dtype=np.float64).reshape(36)
     return float(lib().oracle_cond1_6x6(_p(a)))
+
+
+def green_apply(tau: np.ndarray, shape, c0: np.ndarray, s0: np.ndarray) -> np.ndarray:
+    """Green operator of the reference medium applied to tau[9, N] (x fastest); returns out[9, N]."""
+    n1, n2, n3 = shape
+    t = np.ascontiguousarray(tau, dtype=np.float64).reshape(9, -1)
+    out = np.zeros_like(t)
+    c = np.ascontiguousarray(c0, dtype=np.float64).reshape(81)
+    s = np.ascontiguousarray(s0, dtype=np.float64).reshape(81)
+    rc = lib().oracle_green_apply(_p(t), _p(out), int(n1), int(n2), int(n3), _p(c), _p(s))
+    if rc != 0:
+        raise RuntimeError("oracle_green_apply failed")
+    return out
 
 
 def fft3(x: np.ndarray, sign=-1) -> np.ndarray:

@@ -2053,6 +2053,31 @@ void oracle_fft3(double* data, int ncomp, int n1, int n2, int n3, int sign) {
     long N = (long)n1 * n2 * n3;
     for (int k = 0; k < ncomp; k++) fft3_field(c + k * N, n1, n2, n3, p1, p2, p3);
 }
+int oracle_green_apply(const double* tau9, double* out9, int n1, int n2, int n3, const double* c0, const double* s0) {
+    // form_G (igamma=0) + convolution_with_Goper on a bare grid (various_functions.f90:640-809, 966-1059)
+    try {
+        Oracle o;
+        o.n1 = n1; o.n2 = n2; o.n3 = n3;
+        o.wgt = 1.0 / ((double)n1 * n2 * n3);
+        o.init_micro();
+        o.process.assign(1, Process());
+        o.ipr = 1;
+        std::memcpy(o.c0, c0, sizeof(T4));
+        std::memcpy(o.s0, s0, sizeof(T4));
+        o.form_G();
+        const long N = o.N;
+        for (long v = 0; v < N; v++)
+            for (int c = 0; c < 9; c++) o.vox[v].sgPK1[c / 3][c % 3] = tau9[(long)c * N + v];
+        o.convolution();
+        for (long v = 0; v < N; v++)
+            for (int c = 0; c < 9; c++) out9[(long)c * N + v] = o.vox[v].dvelgradref[c / 3][c % 3];
+    } catch (std::exception& e) {
+        std::fprintf(stderr, "oracle_green_apply: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
 void oracle_plastic_rate(const double* sch5xn, const double* trialtau_nx2, const double* nrs, const double* gamd0, int nsyst,
                          const double* sg6, double* edotp6, double* dedotp66, double* gamdot) {
     Phase ph;

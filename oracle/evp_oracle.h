@@ -62,6 +62,8 @@ double oracle_cond1_6x6(const double* a66);
 /* In-place 3-D DFT of ncomp complex fields (interleaved re,im), x fastest.
  * sign = -1 forward, +1 backward (unnormalised). */
 void oracle_fft3(double* data, int ncomp, int n1, int n2, int n3, int sign);
+/* Green operator (igamma=0) applied to 9 real fields tau9[c*N + v]. 0 = ok. */
+int oracle_green_apply(const double* tau9, double* out9, int n1, int n2, int n3, const double* c0, const double* s0);
 /* One constitutive evaluation (plastic_strain_rate + elastic_strain_rate). */
 void oracle_plastic_rate(const double* sch5xn, const double* trialtau_nx2,
                          const double* nrs, const double* gamd0, int nsyst,
