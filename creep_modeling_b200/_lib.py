@@ -11,7 +11,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_build" / "libevp_b200.so"
 
 EXPORTED = (
     "evp_solve_file", "evp_open", "evp_advance", "evp_get_field", "evp_last_rows", "evp_stats", "evp_close",
-    "evp_kernel_times", "evp_green_apply", "evp_last_error", "evp_version",
+    "evp_kernel_times", "evp_green_apply", "evp_green_apply_noalloc", "evp_last_error", "evp_version",
 )
 
 STATUS = {
@@ -78,6 +78,8 @@ def load(path: Path | str | None = None):
     L.evp_kernel_times.restype = ctypes.c_int
     L.evp_green_apply.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, vp]
     L.evp_green_apply.restype = ctypes.c_int
+    L.evp_green_apply_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, vp]
+    L.evp_green_apply_noalloc.restype = ctypes.c_int
     L.evp_last_error.argtypes = []
     L.evp_last_error.restype = ctypes.c_char_p
     L.evp_version.argtypes = []

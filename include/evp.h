@@ -87,6 +87,22 @@ int evp_kernel_times(evp_solve* s, char* names, long long* launches, double* ms,
 int evp_green_apply(const double* d_tau, double* d_out, int n1, int n2, int n3, const double* c0, const double* s0,
                     void* stream);
 
+/* Allocation-free variant of evp_green_apply (no counterpart in the reference,
+ * whose Fortran solver has no device and no allocator to avoid).  For callers
+ * that cannot call cudaMalloc: their device memory belongs to another
+ * allocator (a pre-reserved pool such as PyTorch's caching allocator, or a
+ * serving loop whose HBM budget is already handed out), or they run
+ * latency-critical loops that cannot take the device-wide synchronization of
+ * cudaMalloc / cudaFree.  Same arguments and results as evp_green_apply; the
+ * scratch lives in a fixed array of about 2.5 MB that every GPU loading this
+ * library keeps until the process exits.  Limits: (n1/2+1)*n2*n3 <= 17408
+ * (a 32^3 grid) and every edge <= 256; larger grids return -7 with a message.
+ * The first call on a device resolves the array's address and should come
+ * before any stream capture.  All calls on a device share the array, so calls
+ * whose device work overlaps race and must be serialized by the caller. */
+int evp_green_apply_noalloc(const double* d_tau, double* d_out, int n1, int n2, int n3, const double* c0,
+                            const double* s0, void* stream);
+
 /* Message of the last failing call on this thread. */
 const char* evp_last_error(void);
 int evp_version(void);
