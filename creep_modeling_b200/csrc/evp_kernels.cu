@@ -403,6 +403,13 @@ __device__ __forceinline__ void constitutive(const PhaseDev& ph, const double* _
         }
     }
 }
+// x[i] for a run-time i in 0..5 without a local-memory array
+__device__ __forceinline__ double sel6(const double (&x)[6], int i) {
+    double y = x[0];
+#pragma unroll
+    for (int c = 1; c < 6; c++) y = (i == c) ? x[c] : y;
+    return y;
+}
 __device__ __forceinline__ double dd_at(const double (&dd)[15], int i, int j) {
     if (i > 4 || j > 4) return 0.0;
     int a = i < j ? i : j, b = i < j ? j : i;
@@ -442,8 +449,8 @@ __device__ __forceinline__ void harden(const PhaseDev& ph, const double* __restr
 }
 
 // ---------------------------------------------------------------- k_newton
-template <int NS>
-__global__ void __launch_bounds__(kNewtonBlock) k_newton(Dev d, NewtonParams p) {
+template <int NS, int MINB>
+__global__ void __launch_bounds__(kNewtonBlock, MINB) k_newton(Dev d, NewtonParams p) {
     const long long N = d.N;
     double s[14];
 #pragma unroll
@@ -644,11 +651,459 @@ __global__ void __launch_bounds__(kNewtonBlock) k_newton(Dev d, NewtonParams p) 
     }
     reduce_store<14, 0>(s, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
 }
+// ---------------------------------------------------------------- k_newton6: six lanes per voxel
+// The local solve of k_newton with the voxel's operators held in registers for
+// the whole Newton solve instead of being re-read from memory at every
+// evaluation.  A warp holds five voxels, one per group of six lanes (lanes 30
+// and 31 hold none).  Lane r of a group owns row r of C~ (c066mod), of the
+// compliance S (sg66), of M = C~ S / dt and, with the augmented Lagrangian,
+// of C~ Gamma (cG); it owns component r of every 6-vector in the b-basis and
+// the slip systems s = r + 6k.  Vectors are exchanged with warp shuffles and
+// group sums are formed in one fixed order, so every lane of a group holds the
+// bitwise-identical sum.  All loops run warp-uniformly (until no group of the
+// warp is still active), with every state update predicated on its group's
+// flag, so the shuffles always use the full warp mask.  The 6x6 Newton system
+// is solved by Gauss-Jordan elimination with partial pivoting (pivot: largest
+// |a| in the column, first row on ties, as dgesv), one row per lane, without
+// moving rows between lanes.  Against k_newton the arithmetic differs only in
+// rounding: the Jacobian is I + C~ dd + M (- cG), sums run in another order
+// and the elimination is Gauss-Jordan.
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ double gsum6(double x, int base) {
+    const double pr = x + __shfl_xor_sync(kFull, x, 1);  // lanes 2j, 2j+1 of a group (groups start at even lanes)
+    const double p0 = __shfl_sync(kFull, pr, base), p1 = __shfl_sync(kFull, pr, base + 2),
+                 p2 = __shfl_sync(kFull, pr, base + 4);
+    return (p0 + p1) + p2;
+}
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a > b ? a : b; }
+
+template <int SPL, bool MODAL, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_newton6(Dev d, NewtonParams p) {
+    const long long N = d.N;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / 6;               // 0..4 hold voxels; group 5 (lanes 30, 31) is idle
+    const int r = lane - 6 * grp;           // row / component owned by this lane
+    const int base = grp < 5 ? 6 * grp : 24;  // idle lanes shadow group 4's lanes and write nothing
+    double acc[14];
+#pragma unroll
+    for (int c = 0; c < 14; c++) acc[c] = 0.0;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const double tolt = fmax(p.error, p.erroral);
+    for (long long v0 = wid * 5; v0 < N; v0 += nwarp * 5) {  // warp-uniform
+        const bool valid = grp < 5 && v0 + grp < N;
+        const long long v = valid ? v0 + grp : v0;  // in-range index for the loads of idle lanes
+        const bool gas = valid && d.gas[v];
+        const bool act = valid && !gas;
+        const double w = d.wgtc[v];
+        if (gas && r == 0) {  // dummy gas voxel: closed-form update by one lane
+            double lam[6], sgt6[6], D6[6], t[6], res[6], out[6], s6v[6], a[6], vg[9], vs[9];
+            ld6(d.sg, N, v, a);
+            s6_to_b6(a, lam);
+            ld6(d.sgt, N, v, a);
+            s6_to_b6(a, sgt6);
+            ld9(d.velgrad, N, v, vg);
+            sym33(vg, vs);
+            t2_to_b6(vs, D6);
+#pragma unroll
+            for (int i = 0; i < 6; i++) t[i] = D6[i] + sgt6[i] / p.tdot * p.complgas;
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double x = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) x += d.c066mod[(6 * i + j) * N + v] * t[j];
+                res[i] = lam[i] + x;
+            }
+            if (MODAL) {
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    double x = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 6; j++) x += d.cG[(6 * i + j) * N + v] * lam[j];
+                    res[i] -= x;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double x = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) x += d.cgas[(6 * i + j) * N + v] * res[j];
+                out[i] = x;
+            }
+            b6_to_s6(out, s6v);
+            st6(d.sg, N, v, s6v);
+#pragma unroll
+            for (int c = 0; c < 6; c++) d.edotp[c * N + v] = 0.0;
+            for (int q = 0; q < d.nsys; q++) d.gamdot[q * N + v] = 0.0;
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc[8 + c] += s6v[c] * w;
+        }
+        // per-voxel vectors: full in every lane while A and q are formed, component r afterwards
+        double lam_r, sgt_r, D_r, eth_r, Crow[6], Arow[6], q_r;
+        const PhaseDev& ph = d.ph[d.phase[v]];
+        const int nsyst = ph.nsyst;
+        {
+        double lamf[6], sgtf[6], Df[6], ethf[6] = {0, 0, 0, 0, 0, 0};
+        {
+            double a[9], vs[9];
+            ld6(d.sg, N, v, a);
+            s6_to_b6(a, lamf);
+            ld6(d.sgt, N, v, a);
+            s6_to_b6(a, sgtf);
+            ld9(d.velgrad, N, v, a);
+            sym33(a, vs);
+            t2_to_b6(vs, Df);
+            if (p.thermo) {
+                ld9(d.eth, N, v, a);
+                t2_to_b6(a, ethf);
+            }
+        }
+        // The residual of solve_res,
+        //   res = sg - lam + C~ (edotp + S (sg - sgt) / dt + eth - D) - cG (sg - lam),
+        // is evaluated as res = A sg + C~ edotp - q with, per voxel,
+        //   A = I + M - cG,  M = C~ S / dt,  q = lam + M sgt + C~ (D - eth) - cG lam,
+        // and the Jacobian is A + C~ dd.  Lane r keeps rows r of C~ and A and q_r.
+        {
+            double Srow[6], M[6];
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                Crow[j] = d.c066mod[(6 * r + j) * N + v];
+                Srow[j] = d.sg66[(6 * r + j) * N + v];
+                M[j] = 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 6; k++)
+#pragma unroll
+                for (int j = 0; j < 6; j++) M[j] += Crow[k] * (__shfl_sync(kFull, Srow[j], base + k) / p.tdot);
+            q_r = sel6(lamf, r);
+            double ms = 0.0, cd = 0.0, gl = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                const double g = MODAL ? d.cG[(6 * r + j) * N + v] : 0.0;
+                Arow[j] = ((r == j) ? 1.0 : 0.0) + M[j] - g;
+                ms += M[j] * sgtf[j];
+                cd += Crow[j] * (Df[j] - ethf[j]);
+                gl += g * lamf[j];
+            }
+            q_r = q_r + ms + cd - gl;
+        }
+        lam_r = sel6(lamf, r);
+        sgt_r = sel6(sgtf, r);
+        D_r = sel6(Df, r);
+        eth_r = sel6(ethf, r);
+        }
+        // slip systems of this lane and their constants
+        double sch[SPL][5], tt[SPL][2], gd[SPL], rs1[SPL], g0s[SPL], nrs[SPL];
+        double taun = 0.0;
+#pragma unroll
+        for (int k = 0; k < SPL; k++) {
+            const int s = r + 6 * k;
+            const bool own = s < nsyst, any = s < d.nsys;
+#pragma unroll
+            for (int c = 0; c < 5; c++) sch[k][c] = own ? d.sch[(s * 5 + c) * N + v] : 0.0;
+            tt[k][0] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
+            tt[k][1] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
+            g0s[k] = own ? ph.gamd0[s] : 0.0;
+            nrs[k] = own ? ph.nrs[s] : 1.0;
+            gd[k] = 0.0;
+            rs1[k] = 0.0;
+            taun += tt[k][0] * tt[k][0] + tt[k][1] * tt[k][1];
+        }
+        const int int_exp = ph.int_exp;
+        taun = sqrt(gsum6(taun, base));
+        double sg_r = lam_r;
+        const double sgnorm = sqrt(gsum6(sg_r * sg_r, base));
+        double sgold_r = 0.0, sev_r = 0.0, edotp_r = 0.0;
+        const double gamma0 = d.gacumgr[v];
+        int itertau = 0;
+        double errtau = 2.0 * tolt;
+        bool aT = act;
+        while (true) {
+            aT = aT && itertau < 10 && errtau > tolt;
+            if (!__any_sync(kFull, aT)) break;
+            itertau += aT;
+            int iterNR = 0;
+            double erral = 2.0 * p.erroral, resoldn = 1.0;
+            bool aN = aT;
+            while (true) {
+                aN = aN && iterNR < 100 && erral > p.erroral;
+                if (!__any_sync(kFull, aN)) break;
+                iterNR += aN;
+                int icut = 0;
+                double resn = 2.0 * resoldn, res_r = 0.0;
+                bool aC = aN;
+                while (true) {
+                    aC = aC && resn > resoldn && icut < 10;
+                    if (!__any_sync(kFull, aC)) break;
+                    // plastic_strain_rate at sg (own systems), summed over the group
+                    double sgf[6];
+#pragma unroll
+                    for (int c = 0; c < 6; c++) sgf[c] = __shfl_sync(kFull, sg_r, base + c);
+                    double ep[5] = {0, 0, 0, 0, 0}, gdn[SPL], rsn[SPL];
+#pragma unroll
+                    for (int k = 0; k < SPL; k++) {
+                        gdn[k] = 0.0;
+                        rsn[k] = 0.0;
+                        if (r + 6 * k < nsyst) {
+                            double rss = sch[k][0] * sgf[0] + sch[k][1] * sgf[1] + sch[k][2] * sgf[2] + sch[k][3] * sgf[3] +
+                                         sch[k][4] * sgf[4];
+                            const double tau = (rss - 0.0 < 0.0) ? tt[k][1] : tt[k][0];
+                            rss = (rss - 0.0) / tau;
+                            const double dum = g0s[k] * powabs(rss, nrs[k] - 1.0, int_exp);
+                            rsn[k] = nrs[k] * dum / tau;
+                            gdn[k] = rss * dum;
+#pragma unroll
+                            for (int c = 0; c < 5; c++) ep[c] += sch[k][c] * gdn[k];
+                        }
+                    }
+                    double rn = -q_r, epr = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 5; c++) {
+                        const double t = gsum6(ep[c], base);
+                        epr = (r == c) ? t : epr;
+                        rn += Crow[c] * t;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 6; j++) rn += Arow[j] * sgf[j];
+                    const double rnn = sqrt(gsum6(rn * rn, base));
+                    if (aC) {
+#pragma unroll
+                        for (int k = 0; k < SPL; k++) {
+                            gd[k] = gdn[k];
+                            rs1[k] = rsn[k];
+                        }
+                        edotp_r = epr;
+                        sev_r = sg_r;
+                        res_r = rn;
+                        resn = rnn;
+                        if (iterNR == 1) resoldn = resn;
+                        if (resn > resoldn) sg_r = sgold_r + (sg_r - sgold_r) * 0.5;
+                        icut++;
+                    }
+                }
+                if (aN) {
+                    resoldn = resn;
+                    sgold_r = sg_r;
+                }
+                // d(edotp)/d(sigma): the 5x5 symmetric sum over the group's systems
+                double dd[15];
+#pragma unroll
+                for (int q = 0; q < 15; q++) dd[q] = 0.0;
+#pragma unroll
+                for (int k = 0; k < SPL; k++) {
+                    if (r + 6 * k < nsyst) {
+                        int q = 0;
+#pragma unroll
+                        for (int jj = 0; jj < 5; jj++)
+#pragma unroll
+                            for (int ii = 0; ii <= jj; ii++) dd[q++] += sch[k][ii] * sch[k][jj] * rs1[k];
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 15; q++) dd[q] = gsum6(dd[q], base);
+                // row r of the Jacobian A + C~ dd
+                double Jr[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                    double x = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 5; k++) x += Crow[k] * dd_at(dd, k, j);
+                    Jr[j] = Arow[j] + x;
+                }
+                // Gauss-Jordan elimination; the low three bits of the pivot key carry 7 - row
+                double b = res_r, dpiv = 1.0;
+                bool sing = false;
+                unsigned usedm = 0u;  // rows already pivoted (group-uniform)
+                int pvs[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    int pv;
+                    if (k < 5) {
+                        unsigned long long key =
+                            ((usedm >> r) & 1u)
+                                ? 0ull
+                                : (((unsigned long long)__double_as_longlong(fabs(Jr[k])) & ~7ull) | (unsigned long long)(7 - r));
+                        key = umax64(key, __shfl_xor_sync(kFull, key, 1));
+                        key = umax64(umax64(__shfl_sync(kFull, key, base), __shfl_sync(kFull, key, base + 2)),
+                                     __shfl_sync(kFull, key, base + 4));
+                        pv = 7 - (int)(key & 7ull);
+                    } else {
+                        pv = __ffs(~usedm & 63u) - 1;  // the one row left
+                    }
+                    pvs[k] = pv;
+                    usedm |= 1u << pv;
+                    const bool me = (r == pv);
+                    double pk[6];
+#pragma unroll
+                    for (int j = k; j < 6; j++) pk[j] = __shfl_sync(kFull, Jr[j], base + pv);
+                    const double bk = __shfl_sync(kFull, b, base + pv);
+                    sing = sing || (pk[k] == 0.0);
+                    const double rinv = 1.0 / pk[k];
+                    if (me) {
+                        dpiv = pk[k];
+                    } else {
+                        const double l = Jr[k] * rinv;
+#pragma unroll
+                        for (int j = k + 1; j < 6; j++) Jr[j] -= l * pk[j];
+                        b -= l * bk;
+                    }
+                }
+                // this lane's row now gives the unknown of the column it pivoted; fetch component r
+                const double xown = b / dpiv;
+                int src = pvs[0];
+#pragma unroll
+                for (int k = 1; k < 6; k++) src = (r == k) ? pvs[k] : src;
+                const double xr = __shfl_sync(kFull, xown, base + src);
+                const double sg_new = sg_r - xr;
+                const double dsgnr = gsum6((sg_new - sgold_r) * (sg_new - sgold_r), base);
+                if (aN) {
+                    if (sing && r == 0) set_err(d.err, 1);
+                    sg_r = sg_new;
+                    erral = sqrt(dsgnr) / sgnorm;
+                }
+            }
+            if (p.iuphard) {  // harden (various_functions.f90:1439-1491)
+                double dg = 0.0;
+#pragma unroll
+                for (int k = 0; k < SPL; k++)
+                    if (r + 6 * k < nsyst) dg += fabs(gd[k]) * p.tdot;
+                const double deltgam = gsum6(dg, base);
+                const double gamma1 = gamma0 + deltgam;
+                double gall[6 * SPL];
+#pragma unroll
+                for (int k = 0; k < SPL; k++)
+#pragma unroll
+                    for (int q = 0; q < 6; q++) gall[6 * k + q] = fabs(__shfl_sync(kFull, gd[k], base + q));
+                double e2 = 0.0, tn[SPL][2];
+#pragma unroll
+                for (int k = 0; k < SPL; k++) {
+                    const int s = r + 6 * k;
+                    tn[k][0] = 0.0;  // systems beyond the phase's own get zero resistance, as harden leaves them
+                    tn[k][1] = 0.0;
+                    if (s < nsyst) {
+                        int mode = 0, last = ph.nsm[0];
+                        while (mode + 1 < ph.nmodes && s >= last) {
+                            mode++;
+                            last += ph.nsm[mode];
+                        }
+                        const double tau1 = ph.tau1[mode], thet0 = ph.thet0[mode], thet1 = ph.thet1[mode];
+                        const double fact = fabs(thet0 / tau1);
+                        const double exp0 = exp(-fact * gamma0), exp1 = exp(-fact * gamma1);
+                        const double voce =
+                            deltgam * thet1 + tau1 * (exp0 - exp1) + thet1 * (gamma0 * exp0 - gamma1 * exp1);
+                        double dtau = 0.0;
+#pragma unroll
+                        for (int js = 0; js < 6 * SPL; js++)
+                            if (js < nsyst) dtau = dtau + ph.hard[s * kMaxSysDev + js] * gall[js];
+                        tn[k][0] = d.crss[(2 * s) * N + v] + dtau * voce * p.tdot / deltgam;
+                        tn[k][1] = d.crss[(2 * s + 1) * N + v] + dtau * voce * p.tdot / deltgam;
+                    }
+                    e2 += (tt[k][0] - tn[k][0]) * (tt[k][0] - tn[k][0]) + (tt[k][1] - tn[k][1]) * (tt[k][1] - tn[k][1]);
+                }
+                const double et = sqrt(gsum6(e2, base)) / taun;
+                if (aT) {
+#pragma unroll
+                    for (int k = 0; k < SPL; k++) {
+                        tt[k][0] = tn[k][0];
+                        tt[k][1] = tn[k][1];
+                    }
+                    errtau = et;
+                }
+            } else if (aT) {
+                errtau = 0.0;
+            }
+        }
+        // |sg - lam|^2 at the final stress; |edot - D|^2 at the last evaluation, with
+        // edot = edotp + S (sg - sgt) / dt + eth as elastic_strain_rate forms it
+        double sgf[6], epf[6], ee = 0.0;
+        {
+            const double ds_r = (sev_r - sgt_r) / p.tdot;
+#pragma unroll
+            for (int j = 0; j < 6; j++) ee += d.sg66[(6 * r + j) * N + v] * __shfl_sync(kFull, ds_r, base + j);
+        }
+        double edot_r = edotp_r + ee;
+        if (p.thermo) edot_r = edot_r + eth_r;
+        const double dl = sg_r - lam_r, de = edot_r - D_r;
+        const double dsgnorm = gsum6(dl * dl, base), ddgnorm = gsum6(de * de, base);
+        // outputs: sigma and edotp in the symmetric 3x3 form, slip rates and resistances
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            sgf[c] = __shfl_sync(kFull, sg_r, base + c);
+            epf[c] = __shfl_sync(kFull, edotp_r, base + c);
+        }
+        epf[5] = 0.0;
+        if (act) {
+            double s6v[6], e6v[6];
+            b6_to_s6(sgf, s6v);
+            b6_to_s6(epf, e6v);
+            d.sg[r * N + v] = sel6(s6v, r);
+            d.edotp[r * N + v] = sel6(e6v, r);
+#pragma unroll
+            for (int k = 0; k < SPL; k++) {
+                const int s = r + 6 * k;
+                if (s < d.nsys) {
+                    d.gamdot[s * N + v] = (s < nsyst) ? gd[k] : 0.0;
+                    d.trialtau[(2 * s) * N + v] = tt[k][0];
+                    d.trialtau[(2 * s + 1) * N + v] = tt[k][1];
+                }
+            }
+            if (r == 0) {
+                if (!(dsgnorm == dsgnorm) || !(ddgnorm == ddgnorm)) set_err(d.err, 2);
+                acc[0] += dsgnorm * w;
+                acc[1] += ddgnorm * w;
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    acc[2 + c] += w * s6v[c];
+                    acc[8 + c] += s6v[c] * w;
+                }
+            }
+        }
+    }
+    reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
+}
+
 void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
-    int grid = (int)((d.N + kNewtonBlock - 1) / kNewtonBlock);
-    if (grid > 148 * 16) grid = 148 * 16;
-    if (d.nsys <= 12) k_newton<12><<<grid, kNewtonBlock, 0, st>>>(d, p);
-    else k_newton<24><<<grid, kNewtonBlock, 0, st>>>(d, p);
+    static const bool legacy = [] {
+        const char* e = getenv("EVP_NEWTON_ONE_THREAD");
+        return e && e[0] == '1';
+    }();
+    if (legacy) {
+        int grid = (int)((d.N + kNewtonBlock - 1) / kNewtonBlock);
+        if (grid > 148 * 16) grid = 148 * 16;
+        static const int mb = [] {
+            const char* e = getenv("EVP_NEWTON_MINB");
+            return e ? atoi(e) : 2;
+        }();
+        if (mb == 6) {
+            if (d.nsys <= 12) k_newton<12, 6><<<grid, kNewtonBlock, 0, st>>>(d, p);
+            else k_newton<24, 6><<<grid, kNewtonBlock, 0, st>>>(d, p);
+        } else {
+            if (d.nsys <= 12) k_newton<12, 2><<<grid, kNewtonBlock, 0, st>>>(d, p);
+            else k_newton<24, 2><<<grid, kNewtonBlock, 0, st>>>(d, p);
+        }
+        return;
+    }
+    const long long warps = (d.N + 4) / 5;
+    long long g = (warps + 7) / 8;  // 8 warps per block of 256
+    const int grid = (int)(g < 148LL * 24 ? g : 148LL * 24);
+    const bool big = d.nsys > 12;
+    static const int minb = [] {
+        const char* e = getenv("EVP_NEWTON6_MINB");
+        return e ? atoi(e) : 2;
+    }();
+#define EVP_N6(MB)                                                        \
+    if (p.modal) {                                                       \
+        if (big) k_newton6<4, true, MB><<<grid, 256, 0, st>>>(d, p);     \
+        else k_newton6<2, true, MB><<<grid, 256, 0, st>>>(d, p);         \
+    } else {                                                             \
+        if (big) k_newton6<4, false, MB><<<grid, 256, 0, st>>>(d, p);    \
+        else k_newton6<2, false, MB><<<grid, 256, 0, st>>>(d, p);        \
+    }
+    if (minb == 3) { EVP_N6(3) }
+    else if (minb == 1) { EVP_N6(1) }
+    else { EVP_N6(2) }
+#undef EVP_N6
 }
 
 // ---------------------------------------------------------------- k_upd1
