@@ -64,6 +64,7 @@ struct Dev {
     double *F, *Finv, *Fe, *Fp, *Finc, *Feinc, *ag;      // 9
     double *detF, *wgtc, *epvm, *gacumgr;                // 1
     double *sg66, *c066mod, *cG, *cgas;                  // 36 (cG, cgas may be null)
+    double *c066inv;                                     // 36: inverse of c066mod, formed with it
     double *sch;                                         // 5*nsys   [(s*5+c)*N + v]
     double *crss, *trialtau;                             // 2*nsys   [(s*2+c)*N + v]
     double *gamdot;                                      // nsys

@@ -19,6 +19,7 @@
 #include "evp_dev.cuh"
 #include "evp_math.cuh"
 
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 
@@ -163,13 +164,6 @@ static int min_radix(const FftPlan1D& pl) {
     int r = 64;
     for (int i = 0; i < pl.nst; i++) r = pl.rad[i] < r ? pl.rad[i] : r;
     return pl.nst ? r : 1;
-}
-static int pick_threads(int P, const FftPlan1D& pl, int want) {
-    const int need = (P * pl.n / min_radix(pl) + 3) / 4;
-    int t = want > need ? want : need;
-    t = (t + 31) / 32 * 32;
-    if (t > 1024) throw std::runtime_error("FFT tile too large");
-    return t;
 }
 
 // ---------------------------------------------------------------- x forward (R2C)
@@ -562,15 +556,40 @@ __global__ void k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ o
 }
 
 // ---------------------------------------------------------------- launchers
+// A pass needs P * n / (smallest radix) / 4 threads for P pencils of length n
+// (four butterflies per thread).  The FFT kernels carry the butterflies of
+// every radix and use many registers, which caps their block size below 1024:
+// each launcher asks the kernel for its limit and shrinks its tile (pencils
+// per block) until the threads fit.
+static int kernel_max_threads(const void* k) {
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, k) != cudaSuccess || a.maxThreadsPerBlock < 32) return 256;
+    return a.maxThreadsPerBlock;
+}
+// largest tile T <= T0 whose ncomp * T pencils fit in maxthr threads; thr gets the block size
+static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int want, int maxthr, int& thr) {
+    for (int T = T0; T >= 1; T--) {
+        const int need = (ncomp * T * pl.n / min_radix(pl) + 3) / 4;
+        int t = want > need ? want : need;
+        t = (t + 31) / 32 * 32;
+        if (t > maxthr) t = maxthr / 32 * 32;
+        if (need <= t) {
+            thr = t;
+            return T;
+        }
+    }
+    throw std::runtime_error("FFT pencils of length " + std::to_string(pl.n) + " do not fit one block");
+}
 static int x_rows_per_block(int n1) { return (256 / n1) > 1 ? 256 / n1 : 1; }
 
 void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
                         double* out, const double* c0, const double* s0, cudaStream_t st) {
-    const int G = x_rows_per_block(d.n1);
+    static const int mx = std::min(kernel_max_threads((const void*)k_green_x_fwd), kernel_max_threads((const void*)k_green_x_inv));
+    int thr = 0;
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const int P = 9 * G;
-    const int thr = pick_threads(P, pl1, 256);
     const size_t smem = (size_t)P * d.n1 * sizeof(double2);
     k_green_x_fwd<<<grid, thr, smem, st>>>(d, pl1, G, tau);
     launch_fft_y(d, pl2, 9, false, st);
@@ -580,11 +599,12 @@ void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
 }
 
 void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
-    const int G = x_rows_per_block(d.n1);
+    static const int mx = kernel_max_threads((const void*)k_fft_x_fwd);
+    int thr = 0;
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl, 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const int P = 9 * G;
-    const int thr = pick_threads(P, pl, 256);
     const size_t smem = (size_t)P * d.n1 * sizeof(double2);
     k_fft_x_fwd<<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
 }
@@ -596,9 +616,10 @@ static int y_tile(const Dev& d) {
     return (d.n1h + nt - 1) / nt;
 }
 void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
-    const int T = y_tile(d);
+    static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true>), kernel_max_threads((const void*)k_fft_y<false>));
+    int thr = 0;
+    const int T = fit_tile(y_tile(d), 1, pl, 128, mx, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
-    const int thr = pick_threads(T, pl, 128);
     const size_t smem = (size_t)T * d.n2 * sizeof(double2);
     if (inverse) k_fft_y<true><<<grid, thr, smem, st>>>(d, pl, T);
     else k_fft_y<false><<<grid, thr, smem, st>>>(d, pl, T);
@@ -611,26 +632,29 @@ static int z_tile(const Dev& d) {
     return (d.n1h + nt - 1) / nt;
 }
 void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
-    const int T = z_tile(d);
+    static const int mx = kernel_max_threads((const void*)k_fft_z_green);
+    int thr = 0;
+    const int T = fit_tile(z_tile(d), 9, pl, 256, mx, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
-    const int thr = pick_threads(9 * T, pl, 256);
     const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
     k_fft_z_green<<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
 }
 void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
-    const int T = z_tile(d);
+    static const int mx = kernel_max_threads((const void*)k_fft_z_integ);
+    int thr = 0;
+    const int T = fit_tile(z_tile(d), 9, pl, 256, mx, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
-    const int thr = pick_threads(9 * T, pl, 256);
     const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
     k_fft_z_integ<<<grid, thr, smem, st>>>(d, pl, T, ideriv);
 }
 void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
-    const int G = x_rows_per_block(d.n1);
+    static const int mx = kernel_max_threads((const void*)k_fft_x_inv);
     const int ncomp = (mode == 0) ? 9 : 3;
+    int thr = 0;
+    const int G = fit_tile(x_rows_per_block(d.n1), ncomp, pl, 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const int P = ncomp * G;
-    const int thr = pick_threads(P, pl, 256);
     const size_t smem = (size_t)P * d.n1 * sizeof(double2);
     k_fft_x_inv<<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
 }

@@ -267,6 +267,14 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __rest
                                     cm[((ii * 3 + jj) * 3 + ll) * 3 + kk] + cm[((jj * 3 + ii) * 3 + ll) * 3 + kk]);
         t4_to_b66(cs, c66);
         for (int c = 0; c < 36; c++) d.c066mod[c * N + v] = c66[c];
+        {  // its inverse, for the symmetric form of the local Newton system
+            double ci[36];
+#pragma unroll
+            for (int c = 0; c < 36; c++) ci[c] = c66[c];
+            if (inv_unrolled<6>(ci) != 0 && !gas) set_err(d.err, 1);
+#pragma unroll
+            for (int c = 0; c < 36; c++) d.c066inv[c * N + v] = ci[c];
+        }
         if (modal) {
             double Fi[9], g66[36];
             ld9(d.Finv, N, v, Fi);
@@ -449,8 +457,8 @@ __device__ __forceinline__ void harden(const PhaseDev& ph, const double* __restr
 }
 
 // ---------------------------------------------------------------- k_newton
-template <int NS, int MINB>
-__global__ void __launch_bounds__(kNewtonBlock, MINB) k_newton(Dev d, NewtonParams p) {
+template <int NS>
+__global__ void __launch_bounds__(kNewtonBlock, 2) k_newton(Dev d, NewtonParams p) {
     const long long N = d.N;
     double s[14];
 #pragma unroll
@@ -678,8 +686,8 @@ __device__ __forceinline__ double gsum6(double x, int base) {
 }
 __device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a > b ? a : b; }
 
-template <int SPL, bool MODAL, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_newton6(Dev d, NewtonParams p) {
+template <int SPL, bool MODAL>
+__global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
     const long long N = d.N;
     const int lane = threadIdx.x & 31;
     const int grp = lane / 6;               // 0..4 hold voxels; group 5 (lanes 30, 31) is idle
@@ -1063,47 +1071,522 @@ __global__ void __launch_bounds__(256, MINB) k_newton6(Dev d, NewtonParams p) {
     reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
 }
 
+// ---------------------------------------------------------------- shared-memory exchange of k_newton6p
+// Group sums and broadcasts go through a per-warp area of shared memory (one
+// 64-bit store or load per double, where a shuffle moves 32 bits).  Rows hold
+// one double per lane at a stride of 33 doubles, so that lanes reading another
+// lane's entries hit distinct banks.  Every write phase starts with
+// __syncwarp(), so a row is never overwritten before all lanes have read it.
+constexpr int kXRows = 16, kXStride = 33;
+struct Xw {
+    double* P;      // [kXRows][kXStride]; row kXRows - 1 serves the scalar sums and gathers
+    int lane, base;
+};
+// group sum in lane order, identical in every lane of the group
+__device__ __forceinline__ double xsum(const Xw& X, double x) {
+    double* row = X.P + (kXRows - 1) * kXStride;
+    __syncwarp();
+    row[X.lane] = x;
+    __syncwarp();
+    const double* q = row + X.base;
+    return ((((q[0] + q[1]) + q[2]) + q[3]) + q[4]) + q[5];
+}
+// the group's six values of x, in every lane of the group
+__device__ __forceinline__ void xgather(const Xw& X, double x, double (&out)[6]) {
+    double* row = X.P + (kXRows - 1) * kXStride;
+    __syncwarp();
+    row[X.lane] = x;
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 6; c++) out[c] = row[X.base + c];
+}
+
+// What the local solve reads of a phase, staged in shared memory once per block.
+struct PhaseN {
+    int nsyst, nmodes, int_exp, nsm[3];
+    double nrs[kMaxSysDev], gamd0[kMaxSysDev];
+    double tau1[3], thet0[3], thet1[3];
+    double hard[kMaxSysDev * kMaxSysDev];
+};
+constexpr int kMaxPhaseSmem = 4;
+
+// Dynamic shared memory of k_newton6p: the staged phases, then per warp the
+// exchange rows, the lanes' columns (Schmid vectors 5 * SPL, resistances
+// crss 2 * SPL, accumulated shear 1; rows of kXStride doubles) and the five
+// groups' sums (70).
+__host__ __device__ constexpr int newton6p_col_rows(int spl) { return 7 * spl + 1; }
+__host__ __device__ constexpr int newton6p_warp_doubles(int spl) {
+    return kXRows * kXStride + newton6p_col_rows(spl) * kXStride + 70;
+}
+__host__ __device__ constexpr size_t newton6p_smem_bytes(int spl, int nph) {
+    return (size_t)nph * sizeof(PhaseN) + 8 * sizeof(double) * (size_t)newton6p_warp_doubles(spl);
+}
+
+// ---------------------------------------------------------------- k_newton6p: symmetric positive definite form
+// The local solve without the augmented-Lagrangian term (the modal path uses
+// k_newton6), with the Newton system put in symmetric form.  With
+// dedot = dd + S / dt the Jacobian of solve_res is
+//   J = I + C~ (S / dt + dd) = C~ H,   H = C~^-1 + S / dt + dd,
+// where C~ (c066mod) and S (sg66) are symmetric positive definite and dd is
+// positive semi-definite, so H is symmetric positive definite.  The Newton
+// step J^-1 res equals H^-1 rho with rho = C~^-1 res, and rho is formed
+// directly:
+//   rho = H0 sg + edotp - q',  H0 = C~^-1 + S / dt,  q' = C~^-1 lam + (S / dt) sgt + D - eth,
+// while res = C~ rho gives the residual norm that drives the step halving.
+// Elimination on H needs no pivoting: lanes eliminate in the fixed order
+// 0..5 (Gauss-Jordan), and lane r ends with the unknown of column r; lane r
+// reads only row r of dd.  Against dgesv on J the Newton step differs in
+// rounding only.  Five voxels per warp, six lanes per voxel as in k_newton6;
+// the Schmid vectors, resistances and the per-group sums live in shared
+// memory, which keeps the kernel within 128 registers (16 warps per SM).
+template <int SPL>
+__global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
+    extern __shared__ double dyn_smem[];
+    PhaseN* const sph = reinterpret_cast<PhaseN*>(dyn_smem);
+    const int nph = d.nph < kMaxPhaseSmem ? d.nph : kMaxPhaseSmem;
+    for (int q = threadIdx.x; q < nph; q += blockDim.x) {
+        const PhaseDev& g = d.ph[q];
+        sph[q].nsyst = g.nsyst;
+        sph[q].nmodes = g.nmodes;
+        sph[q].int_exp = g.int_exp;
+        for (int m = 0; m < 3; m++) {
+            sph[q].nsm[m] = g.nsm[m];
+            sph[q].tau1[m] = g.tau1[m];
+            sph[q].thet0[m] = g.thet0[m];
+            sph[q].thet1[m] = g.thet1[m];
+        }
+    }
+    for (int e = threadIdx.x; e < nph * kMaxSysDev; e += blockDim.x) {
+        sph[e / kMaxSysDev].nrs[e % kMaxSysDev] = d.ph[e / kMaxSysDev].nrs[e % kMaxSysDev];
+        sph[e / kMaxSysDev].gamd0[e % kMaxSysDev] = d.ph[e / kMaxSysDev].gamd0[e % kMaxSysDev];
+    }
+    for (int e = threadIdx.x; e < nph * kMaxSysDev * kMaxSysDev; e += blockDim.x)
+        sph[e / (kMaxSysDev * kMaxSysDev)].hard[e % (kMaxSysDev * kMaxSysDev)] =
+            d.ph[e / (kMaxSysDev * kMaxSysDev)].hard[e % (kMaxSysDev * kMaxSysDev)];
+    __syncthreads();
+    double* const wsm = reinterpret_cast<double*>(sph + nph) + (threadIdx.x >> 5) * newton6p_warp_doubles(SPL);
+    const long long N = d.N;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / 6;                 // 0..4 hold voxels; group 5 (lanes 30, 31) is idle
+    const int r = lane - 6 * grp;             // row / component owned by this lane
+    const int base = grp < 5 ? 6 * grp : 24;  // idle lanes shadow group 4's lanes and write nothing
+    const Xw X{wsm, lane, base};
+    // this lane's column: Schmid vectors, resistances, accumulated shear
+    double* const schm = wsm + kXRows * kXStride + lane;
+    double* const crsm = schm + 5 * SPL * kXStride;
+    double* const gam0 = schm + 7 * SPL * kXStride;
+    double* const accw = wsm + kXRows * kXStride + newton6p_col_rows(SPL) * kXStride;
+    for (int c = lane; c < 70; c += 32) accw[c] = 0.0;
+    __syncwarp();
+    double* const accg = accw + (grp < 5 ? grp : 0) * 14;
+    const double tolt = fmax(p.error, p.erroral);
+    // position of dd(r, j) in the packed upper triangle, for this lane's row
+    int ddq[5];
+#pragma unroll
+    for (int j = 0; j < 5; j++) ddq[j] = (r < j) ? j * (j + 1) / 2 + r : r * (r + 1) / 2 + j;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v0 = wid * 5; v0 < N; v0 += nwarp * 5) {  // warp-uniform
+        const bool valid = grp < 5 && v0 + grp < N;
+        const long long v = valid ? v0 + grp : v0;  // in-range index for the loads of idle lanes
+        const bool gasv = d.gas[v];
+        const int phi = d.phase[v];
+        // rows r of C~ and H0, q'_r and this lane's systems; no load waits on the gas flag or phase
+        double lam_r, Crow[6], Hrow[6], qp_r, tt[SPL][2];
+        {
+            double lamf[6], sgtf[6], a[9], b6[6], vs[9];
+            ld6(d.sg, N, v, a);
+            s6_to_b6(a, lamf);
+            ld6(d.sgt, N, v, a);
+            s6_to_b6(a, sgtf);
+            ld9(d.velgrad, N, v, a);
+            sym33(a, vs);
+            t2_to_b6(vs, b6);
+            double De = sel6(b6, r);
+            if (p.thermo) {
+                ld9(d.eth, N, v, a);
+                t2_to_b6(a, b6);
+                De = De - sel6(b6, r);
+            }
+            double cl = 0.0, ss = 0.0;
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                Crow[j] = d.c066mod[(6 * r + j) * N + v];
+                const double ci = d.c066inv[(6 * r + j) * N + v];
+                const double sd = d.sg66[(6 * r + j) * N + v] / p.tdot;
+                Hrow[j] = ci + sd;
+                cl += ci * lamf[j];
+                ss += sd * sgtf[j];
+            }
+            qp_r = cl + ss + De;
+            lam_r = sel6(lamf, r);
+#pragma unroll
+            for (int k = 0; k < SPL; k++) {
+                const int s = r + 6 * k;
+                const bool any = s < d.nsys;
+#pragma unroll
+                for (int c = 0; c < 5; c++) schm[(5 * k + c) * kXStride] = any ? d.sch[(s * 5 + c) * N + v] : 0.0;
+                tt[k][0] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
+                tt[k][1] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
+                crsm[(2 * k) * kXStride] = any ? d.crss[(2 * s) * N + v] : 0.0;
+                crsm[(2 * k + 1) * kXStride] = any ? d.crss[(2 * s + 1) * N + v] : 0.0;
+            }
+            *gam0 = d.gacumgr[v];
+        }
+        const PhaseN& ph = sph[phi];
+        const int nsyst = ph.nsyst;
+        const bool gas = valid && gasv;
+        const bool act = valid && !gas;
+        double gd[SPL], rs1[SPL], g0s[SPL], nrs[SPL];
+        double taun = 0.0;
+#pragma unroll
+        for (int k = 0; k < SPL; k++) {
+            const int s = r + 6 * k;
+            const bool own = s < nsyst;
+            if (!own)
+#pragma unroll
+                for (int c = 0; c < 5; c++) schm[(5 * k + c) * kXStride] = 0.0;
+            g0s[k] = own ? ph.gamd0[s] : 0.0;
+            nrs[k] = own ? ph.nrs[s] : 1.0;
+            gd[k] = 0.0;
+            rs1[k] = 0.0;
+            taun += tt[k][0] * tt[k][0] + tt[k][1] * tt[k][1];
+        }
+        const int int_exp = ph.int_exp;
+        taun = sqrt(xsum(X, taun));
+        double sg_r = lam_r;
+        const double sgnorm = sqrt(xsum(X, sg_r * sg_r));
+        double sgold_r = 0.0, sev_r = 0.0, edotp_r = 0.0;
+        int itertau = 0;
+        double errtau = 2.0 * tolt;
+        bool aT = act;
+        while (true) {
+            aT = aT && itertau < 10 && errtau > tolt;
+            if (!__any_sync(kFull, aT)) break;
+            itertau += aT;
+            int iterNR = 0;
+            double erral = 2.0 * p.erroral, resoldn = 1.0;
+            bool aN = aT;
+            while (true) {
+                aN = aN && iterNR < 100 && erral > p.erroral;
+                if (!__any_sync(kFull, aN)) break;
+                iterNR += aN;
+                int icut = 0;
+                double resn = 2.0 * resoldn, rho_c = 0.0;
+                bool aC = aN;
+                while (true) {
+                    aC = aC && resn > resoldn && icut < 10;
+                    if (!__any_sync(kFull, aC)) break;
+                    // plastic_strain_rate at sg (own systems)
+                    double sgf[6];
+                    xgather(X, sg_r, sgf);
+                    double ep[5] = {0, 0, 0, 0, 0}, gdn[SPL], rsn[SPL];
+#pragma unroll
+                    for (int k = 0; k < SPL; k++) {
+                        gdn[k] = 0.0;
+                        rsn[k] = 0.0;
+                        if (r + 6 * k < nsyst) {
+                            double sc[5];
+#pragma unroll
+                            for (int c = 0; c < 5; c++) sc[c] = schm[(5 * k + c) * kXStride];
+                            double rss = sc[0] * sgf[0] + sc[1] * sgf[1] + sc[2] * sgf[2] + sc[3] * sgf[3] + sc[4] * sgf[4];
+                            const double tau = (rss - 0.0 < 0.0) ? tt[k][1] : tt[k][0];
+                            rss = (rss - 0.0) / tau;
+                            const double dum = g0s[k] * powabs(rss, nrs[k] - 1.0, int_exp);
+                            rsn[k] = nrs[k] * dum / tau;
+                            gdn[k] = rss * dum;
+#pragma unroll
+                            for (int c = 0; c < 5; c++) ep[c] += sc[c] * gdn[k];
+                        }
+                    }
+                    // component r of edotp: row r summed over the group in lane order
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < 5; c++) X.P[c * kXStride + lane] = ep[c];
+                    __syncwarp();
+                    double epr = 0.0;
+                    if (r < 5) {
+                        const double* e = X.P + r * kXStride + base;
+                        epr = ((((e[0] + e[1]) + e[2]) + e[3]) + e[4]) + e[5];
+                    }
+                    double rho = epr - qp_r;
+#pragma unroll
+                    for (int j = 0; j < 6; j++) rho += Hrow[j] * sgf[j];
+                    double rhof[6];
+                    xgather(X, rho, rhof);
+                    double rn = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 6; j++) rn += Crow[j] * rhof[j];
+                    const double rnn = sqrt(xsum(X, rn * rn));
+                    if (aC) {
+#pragma unroll
+                        for (int k = 0; k < SPL; k++) {
+                            gd[k] = gdn[k];
+                            rs1[k] = rsn[k];
+                        }
+                        edotp_r = epr;
+                        sev_r = sg_r;
+                        rho_c = rho;
+                        resn = rnn;
+                        if (iterNR == 1) resoldn = resn;
+                        if (resn > resoldn) sg_r = sgold_r + (sg_r - sgold_r) * 0.5;
+                        icut++;
+                    }
+                }
+                if (aN) {
+                    resoldn = resn;
+                    sgold_r = sg_r;
+                }
+                // d(edotp)/d(sigma), packed upper triangle, partial over this lane's systems
+                __syncwarp();
+                {
+                    double sc[SPL][5];
+#pragma unroll
+                    for (int k = 0; k < SPL; k++)
+#pragma unroll
+                        for (int c = 0; c < 5; c++) sc[k][c] = schm[(5 * k + c) * kXStride];
+                    int q = 0;
+#pragma unroll
+                    for (int jj = 0; jj < 5; jj++)
+#pragma unroll
+                        for (int ii = 0; ii <= jj; ii++) {
+                            double x = 0.0;
+#pragma unroll
+                            for (int k = 0; k < SPL; k++)
+                                if (r + 6 * k < nsyst) x += sc[k][ii] * sc[k][jj] * rs1[k];
+                            X.P[q * kXStride + lane] = x;
+                            q++;
+                        }
+                }
+                __syncwarp();
+                // row r of H = H0 + dd (dd summed over the group in lane order)
+                double Hr[6];
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                    double x = 0.0;
+                    if (j < 5 && r < 5) {
+                        const double* e = X.P + ddq[j] * kXStride + base;
+                        x = ((((e[0] + e[1]) + e[2]) + e[3]) + e[4]) + e[5];
+                    }
+                    Hr[j] = Hrow[j] + x;
+                }
+                // Gauss-Jordan elimination in the fixed order 0..5 (H is positive definite)
+                double b = rho_c;
+                bool sing = false;
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    double pk[6];
+#pragma unroll
+                    for (int j = k; j < 6; j++) pk[j] = __shfl_sync(kFull, Hr[j], base + k);
+                    const double bk = __shfl_sync(kFull, b, base + k);
+                    sing = sing || (pk[k] == 0.0);
+                    if (r != k) {
+                        const double l = Hr[k] / pk[k];
+#pragma unroll
+                        for (int j = k + 1; j < 6; j++) Hr[j] -= l * pk[j];
+                        b -= l * bk;
+                    }
+                }
+                const double sg_new = sg_r - b / sel6(Hr, r);
+                const double dsgnr = xsum(X, (sg_new - sgold_r) * (sg_new - sgold_r));
+                if (aN) {
+                    if (sing && r == 0) set_err(d.err, 1);
+                    sg_r = sg_new;
+                    erral = sqrt(dsgnr) / sgnorm;
+                }
+            }
+            if (p.iuphard) {  // harden (various_functions.f90:1439-1491)
+                double dg = 0.0;
+#pragma unroll
+                for (int k = 0; k < SPL; k++)
+                    if (r + 6 * k < nsyst) dg += fabs(gd[k]) * p.tdot;
+                const double deltgam = xsum(X, dg);
+                const double gamma0 = *gam0;
+                const double gamma1 = gamma0 + deltgam;
+                double gall[6 * SPL];
+#pragma unroll
+                for (int k = 0; k < SPL; k++) {
+                    double t6[6];
+                    xgather(X, fabs(gd[k]), t6);
+#pragma unroll
+                    for (int q = 0; q < 6; q++) gall[6 * k + q] = t6[q];
+                }
+                double e2 = 0.0, tn[SPL][2];
+#pragma unroll
+                for (int k = 0; k < SPL; k++) {
+                    const int s = r + 6 * k;
+                    tn[k][0] = 0.0;  // systems beyond the phase's own get zero resistance, as harden leaves them
+                    tn[k][1] = 0.0;
+                    if (s < nsyst) {
+                        int mode = 0, last = ph.nsm[0];
+                        while (mode + 1 < ph.nmodes && s >= last) {
+                            mode++;
+                            last += ph.nsm[mode];
+                        }
+                        const double tau1 = ph.tau1[mode], thet0 = ph.thet0[mode], thet1 = ph.thet1[mode];
+                        const double fact = fabs(thet0 / tau1);
+                        const double exp0 = exp(-fact * gamma0), exp1 = exp(-fact * gamma1);
+                        const double voce =
+                            deltgam * thet1 + tau1 * (exp0 - exp1) + thet1 * (gamma0 * exp0 - gamma1 * exp1);
+                        double dtau = 0.0;
+#pragma unroll
+                        for (int js = 0; js < 6 * SPL; js++)
+                            if (js < nsyst) dtau = dtau + ph.hard[s * kMaxSysDev + js] * gall[js];
+                        tn[k][0] = crsm[(2 * k) * kXStride] + dtau * voce * p.tdot / deltgam;
+                        tn[k][1] = crsm[(2 * k + 1) * kXStride] + dtau * voce * p.tdot / deltgam;
+                    }
+                    e2 += (tt[k][0] - tn[k][0]) * (tt[k][0] - tn[k][0]) + (tt[k][1] - tn[k][1]) * (tt[k][1] - tn[k][1]);
+                }
+                const double et = sqrt(xsum(X, e2)) / taun;
+                if (aT) {
+#pragma unroll
+                    for (int k = 0; k < SPL; k++) {
+                        tt[k][0] = tn[k][0];
+                        tt[k][1] = tn[k][1];
+                    }
+                    errtau = et;
+                }
+            } else if (aT) {
+                errtau = 0.0;
+            }
+        }
+        // |sg - lam|^2 at the final stress; |edot - D|^2 at the last evaluation, with
+        // edot = edotp + S (sg - sgt) / dt + eth as elastic_strain_rate forms it
+        double sgf[6], epf[6], ee = 0.0, sgt_r, D_r, eth_r = 0.0;
+        {
+            double a[9], b6[6], vs[9];
+            ld6(d.sgt, N, v, a);
+            s6_to_b6(a, b6);
+            sgt_r = sel6(b6, r);
+            ld9(d.velgrad, N, v, a);
+            sym33(a, vs);
+            t2_to_b6(vs, b6);
+            D_r = sel6(b6, r);
+            if (p.thermo) {
+                ld9(d.eth, N, v, a);
+                t2_to_b6(a, b6);
+                eth_r = sel6(b6, r);
+            }
+        }
+        {
+            double dsf[6];
+            xgather(X, (sev_r - sgt_r) / p.tdot, dsf);
+#pragma unroll
+            for (int j = 0; j < 6; j++) ee += d.sg66[(6 * r + j) * N + v] * dsf[j];
+        }
+        double edot_r = edotp_r + ee;
+        if (p.thermo) edot_r = edot_r + eth_r;
+        const double dl = sg_r - lam_r, de = edot_r - D_r;
+        const double dsgnorm = xsum(X, dl * dl), ddgnorm = xsum(X, de * de);
+        // outputs: sigma and edotp in the symmetric 3x3 form, slip rates and resistances
+        xgather(X, sg_r, sgf);
+        xgather(X, edotp_r, epf);
+        epf[5] = 0.0;
+        if (act) {
+            double s6v[6], e6v[6];
+            b6_to_s6(sgf, s6v);
+            b6_to_s6(epf, e6v);
+            d.sg[r * N + v] = sel6(s6v, r);
+            d.edotp[r * N + v] = sel6(e6v, r);
+#pragma unroll
+            for (int k = 0; k < SPL; k++) {
+                const int s = r + 6 * k;
+                if (s < d.nsys) {
+                    d.gamdot[s * N + v] = (s < nsyst) ? gd[k] : 0.0;
+                    d.trialtau[(2 * s) * N + v] = tt[k][0];
+                    d.trialtau[(2 * s + 1) * N + v] = tt[k][1];
+                }
+            }
+            if (r == 0) {
+                const double w = d.wgtc[v];
+                if (!(dsgnorm == dsgnorm) || !(ddgnorm == ddgnorm)) set_err(d.err, 2);
+                accg[0] += dsgnorm * w;
+                accg[1] += ddgnorm * w;
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    accg[2 + c] += w * s6v[c];
+                    accg[8 + c] += s6v[c] * w;
+                }
+            }
+        }
+        __syncwarp();  // every lane of a gas voxel's group has read sg before the update below writes it
+        if (gas && r == 0) {  // dummy gas voxel: closed-form update by one lane
+            const double w = d.wgtc[v];
+            double lam[6], sgt6[6], D6[6], t[6], res[6], out[6], s6v[6], a[6], vg[9], vs[9];
+            ld6(d.sg, N, v, a);
+            s6_to_b6(a, lam);
+            ld6(d.sgt, N, v, a);
+            s6_to_b6(a, sgt6);
+            ld9(d.velgrad, N, v, vg);
+            sym33(vg, vs);
+            t2_to_b6(vs, D6);
+#pragma unroll
+            for (int i = 0; i < 6; i++) t[i] = D6[i] + sgt6[i] / p.tdot * p.complgas;
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double x = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) x += d.c066mod[(6 * i + j) * N + v] * t[j];
+                res[i] = lam[i] + x;
+            }
+#pragma unroll
+            for (int i = 0; i < 6; i++) {
+                double x = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; j++) x += d.cgas[(6 * i + j) * N + v] * res[j];
+                out[i] = x;
+            }
+            b6_to_s6(out, s6v);
+            st6(d.sg, N, v, s6v);
+#pragma unroll
+            for (int c = 0; c < 6; c++) d.edotp[c * N + v] = 0.0;
+            for (int q = 0; q < d.nsys; q++) d.gamdot[q * N + v] = 0.0;
+#pragma unroll
+            for (int c = 0; c < 6; c++) accg[8 + c] += s6v[c] * w;
+        }
+    }
+    __syncwarp();
+    double acc[14];
+#pragma unroll
+    for (int c = 0; c < 14; c++) acc[c] = lane < 5 ? accw[lane * 14 + c] : 0.0;
+    reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
+}
+
 void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
-    static const bool legacy = [] {
+    // EVP_NEWTON_ONE_THREAD=1 selects the one-thread-per-voxel kernel, kept for comparison
+    static const bool one_thread = [] {
         const char* e = getenv("EVP_NEWTON_ONE_THREAD");
         return e && e[0] == '1';
     }();
-    if (legacy) {
+    const bool big = d.nsys > 12;
+    if (one_thread) {
         int grid = (int)((d.N + kNewtonBlock - 1) / kNewtonBlock);
         if (grid > 148 * 16) grid = 148 * 16;
-        static const int mb = [] {
-            const char* e = getenv("EVP_NEWTON_MINB");
-            return e ? atoi(e) : 2;
-        }();
-        if (mb == 6) {
-            if (d.nsys <= 12) k_newton<12, 6><<<grid, kNewtonBlock, 0, st>>>(d, p);
-            else k_newton<24, 6><<<grid, kNewtonBlock, 0, st>>>(d, p);
-        } else {
-            if (d.nsys <= 12) k_newton<12, 2><<<grid, kNewtonBlock, 0, st>>>(d, p);
-            else k_newton<24, 2><<<grid, kNewtonBlock, 0, st>>>(d, p);
-        }
+        if (big) k_newton<24><<<grid, kNewtonBlock, 0, st>>>(d, p);
+        else k_newton<12><<<grid, kNewtonBlock, 0, st>>>(d, p);
         return;
     }
     const long long warps = (d.N + 4) / 5;
-    long long g = (warps + 7) / 8;  // 8 warps per block of 256
+    const long long g = (warps + 7) / 8;  // 8 warps per block of 256
     const int grid = (int)(g < 148LL * 24 ? g : 148LL * 24);
-    const bool big = d.nsys > 12;
-    static const int minb = [] {
-        const char* e = getenv("EVP_NEWTON6_MINB");
-        return e ? atoi(e) : 2;
-    }();
-#define EVP_N6(MB)                                                        \
-    if (p.modal) {                                                       \
-        if (big) k_newton6<4, true, MB><<<grid, 256, 0, st>>>(d, p);     \
-        else k_newton6<2, true, MB><<<grid, 256, 0, st>>>(d, p);         \
-    } else {                                                             \
-        if (big) k_newton6<4, false, MB><<<grid, 256, 0, st>>>(d, p);    \
-        else k_newton6<2, false, MB><<<grid, 256, 0, st>>>(d, p);        \
+    if (!p.modal && d.nph <= kMaxPhaseSmem) {
+        const size_t sm = newton6p_smem_bytes(big ? 4 : 2, d.nph);
+        if (big) {
+            cudaFuncSetAttribute(k_newton6p<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_newton6p<4><<<grid, 256, sm, st>>>(d, p);
+        } else {
+            cudaFuncSetAttribute(k_newton6p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_newton6p<2><<<grid, 256, sm, st>>>(d, p);
+        }
+        return;
     }
-    if (minb == 3) { EVP_N6(3) }
-    else if (minb == 1) { EVP_N6(1) }
-    else { EVP_N6(2) }
-#undef EVP_N6
+    if (p.modal) {
+        if (big) k_newton6<4, true><<<grid, 256, 0, st>>>(d, p);
+        else k_newton6<2, true><<<grid, 256, 0, st>>>(d, p);
+    } else {
+        if (big) k_newton6<4, false><<<grid, 256, 0, st>>>(d, p);
+        else k_newton6<2, false><<<grid, 256, 0, st>>>(d, p);
+    }
 }
 
 // ---------------------------------------------------------------- k_upd1

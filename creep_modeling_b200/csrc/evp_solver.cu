@@ -267,7 +267,7 @@ public:
         d.F = dalloc<double>(9 * N); d.Finv = dalloc<double>(9 * N); d.Fe = dalloc<double>(9 * N); d.Fp = dalloc<double>(9 * N);
         d.Finc = dalloc<double>(9 * N); d.Feinc = dalloc<double>(9 * N); d.ag = dalloc<double>(9 * N);
         d.detF = dalloc<double>(N); d.wgtc = dalloc<double>(N); d.epvm = dalloc<double>(N); d.gacumgr = dalloc<double>(N);
-        d.sg66 = dalloc<double>(36 * N); d.c066mod = dalloc<double>(36 * N);
+        d.sg66 = dalloc<double>(36 * N); d.c066mod = dalloc<double>(36 * N); d.c066inv = dalloc<double>(36 * N);
         d.cG = dalloc<double>(36 * N);
         d.cgas = dk.has_gas ? dalloc<double>(36 * N) : nullptr;
         d.sch = dalloc<double>(5 * (size_t)ns * N);
@@ -281,7 +281,9 @@ public:
         d.tw1 = dalloc<double2>(dk.n1); d.tw2 = dalloc<double2>(dk.n2); d.tw3 = dalloc<double2>(dk.n3);
         d.dv3 = dalloc<double>(3 * N);
         d.xnode = dalloc<double>(3 * (size_t)(dk.n1 + 1) * (dk.n2 + 1) * d.n3node);
-        d.partials = dalloc<double>(200 * 2048);
+        // block partials: voxel kernels (<= 1184 blocks x 117 sums), Newton (<= 3552 x 14), and the
+        // x inverse pass (one block per <= 1 pair of rows x 9 sums)
+        d.partials = dalloc<double>(std::max<size_t>(200 * 2048, 9 * ((size_t)dk.n2 * dk.n3 / 2 + 1)));
         d.red = dalloc<double>(RED_OUT_SIZE);
         d.counters = dalloc<unsigned int>(CNT_N);
         d.err = dalloc<int>(1);

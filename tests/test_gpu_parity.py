@@ -66,3 +66,15 @@ def test_nonpow2_grid_parity(tmp_path):
     g, o, rg, ro, dg, do = parity.run_both(fft, 3)
     parity.assert_rows_match(rg, ro, dg, do)
     assert parity.field_rel_err(g, o, "velgrad") <= parity.RTOL
+
+
+def test_long_z_pencils_parity(tmp_path):
+    """A 16 x 8 x 48 grid: the z pass would want more threads per block than its
+    kernel allows (81 pencils of length 48), so the launcher shrinks the tile."""
+    case = decks.case_c2(nsteps=2, n=16, ngrains=12)
+    case.n = (16, 8, 48)
+    fft = _case(tmp_path, case)
+    g, o, rg, ro, dg, do = parity.run_both(fft, 2)
+    parity.assert_rows_match(rg, ro, dg, do)
+    for f in ("sg", "velgrad", "gamdot", "xnode"):
+        assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
