@@ -78,9 +78,8 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], const double2* __rest
 
 // One Stockham stage over P pencils of length n stored element-major in
 // shared memory: element e of pencil p at s[e*ES + p].
-template <int R, bool INV>
+template <int R, bool INV, int MAXB>
 __device__ __forceinline__ void fft_stage(double2* s, int ES, int P, int n, int Ns, const double2* __restrict__ tw) {
-    constexpr int MAXB = 4;
     const int nb = n / R, total = nb * P;
     double2 v[MAXB][R];
 #pragma unroll
@@ -114,21 +113,35 @@ __device__ __forceinline__ void fft_stage(double2* s, int ES, int P, int n, int 
     __syncthreads();
 }
 
-template <bool INV>
+// Radix sets: RS = 0 compiles the power-of-two radices only (2, 4, 8; two
+// butterflies per thread), RS = 1 every radix (four butterflies per thread).
+// The power-of-two kernels fit 128 registers, so two blocks of 256 threads
+// are resident per SM where the all-radix kernels (255 registers) allow one.
+template <int RS>
+__host__ __device__ constexpr int fft_maxb() { return RS == 0 ? 2 : 4; }
+
+template <bool INV, int RS>
 __device__ void fft_run(double2* s, int ES, int P, const FftPlan1D& pl, const double2* __restrict__ tw) {
+    constexpr int MB = fft_maxb<RS>();
     int Ns = 1;
     for (int st = 0; st < pl.nst; st++) {
         const int R = pl.rad[st];
         switch (R) {
-            case 2: fft_stage<2, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 3: fft_stage<3, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 4: fft_stage<4, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 5: fft_stage<5, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 7: fft_stage<7, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 8: fft_stage<8, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 11: fft_stage<11, INV>(s, ES, P, pl.n, Ns, tw); break;
-            case 13: fft_stage<13, INV>(s, ES, P, pl.n, Ns, tw); break;
-            default: break;
+            case 2: fft_stage<2, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+            case 4: fft_stage<4, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+            case 8: fft_stage<8, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+            default:
+                if constexpr (RS != 0) {
+                    switch (R) {
+                        case 3: fft_stage<3, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+                        case 5: fft_stage<5, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+                        case 7: fft_stage<7, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+                        case 11: fft_stage<11, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+                        case 13: fft_stage<13, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+                        default: break;
+                    }
+                }
+                break;
         }
         Ns *= R;
     }
@@ -168,7 +181,8 @@ static int min_radix(const FftPlan1D& pl) {
 
 // ---------------------------------------------------------------- x forward (R2C)
 // mode 0: P'_ij = J * ((sigma - <sigma>) F^{-T})_ij ; mode 1: (L F)_ij (grid update)
-__global__ void k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
@@ -210,7 +224,7 @@ __global__ void k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
         for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = val[c];
     }
     __syncthreads();
-    fft_run<false>(s, P, P, pl, d.tw1);
+    fft_run<false, RS>(s, P, P, pl, d.tw1);
     // unpack the two real rows of every pencil
     for (int idx = threadIdx.x; idx < P * n1h; idx += blockDim.x) {
         const int k = idx % n1h, p = idx / n1h;
@@ -227,8 +241,8 @@ __global__ void k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
 }
 
 // ---------------------------------------------------------------- y (C2C)
-template <bool INV>
-__global__ void k_fft_y(Dev d, FftPlan1D pl, int T) {
+template <bool INV, int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_y(Dev d, FftPlan1D pl, int T) {
     extern __shared__ double2 s[];
     const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
     const int kx0 = blockIdx.x * T, k3 = blockIdx.y, c = blockIdx.z;
@@ -238,7 +252,7 @@ __global__ void k_fft_y(Dev d, FftPlan1D pl, int T) {
         s[j * T + t] = (kx < n1h) ? base[(long long)j * n1h + kx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    fft_run<INV>(s, T, T, pl, d.tw2);
+    fft_run<INV, RS>(s, T, T, pl, d.tw2);
     for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
         const int t = idx % T, j = idx / T, kx = kx0 + t;
         if (kx < n1h) base[(long long)j * n1h + kx] = s[j * T + t];
@@ -251,7 +265,8 @@ __device__ __forceinline__ double xi_of(int k, int n) {
     return (k + 1 <= n / 2) ? twopi * (double)k / (double)n : twopi * (double)(k - n) / (double)n;
 }
 
-__global__ void k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
     extern __shared__ double2 s[];
     __shared__ double c0[81], s0[81];
     const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
@@ -264,7 +279,7 @@ __global__ void k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restri
         s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    fft_run<false>(s, P, P, pl, d.tw3);
+    fft_run<false, RS>(s, P, P, pl, d.tw3);
     const bool nyq_y = (n2 % 2 == 0 && j == n2 / 2);
     const double xiy = xi_of(j, n2);
     for (int idx = threadIdx.x; idx < T * n3; idx += blockDim.x) {
@@ -331,7 +346,7 @@ __global__ void k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restri
         for (int c = 0; c < 9; c++) q[c * T] = r[c];
     }
     __syncthreads();
-    fft_run<true>(s, P, P, pl, d.tw3);
+    fft_run<true, RS>(s, P, P, pl, d.tw3);
     for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
         const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
         if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
@@ -339,7 +354,8 @@ __global__ void k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restri
 }
 
 // ---------------------------------------------------------------- z fused with the spectral integration (grid update)
-__global__ void k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
     const int kx0 = blockIdx.x * T, j = blockIdx.y;
@@ -350,7 +366,7 @@ __global__ void k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
         s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    fft_run<false>(s, P, P, pl, d.tw3);
+    fft_run<false, RS>(s, P, P, pl, d.tw3);
     if (blockIdx.x == 0 && j == 0 && threadIdx.x < 9) {
         const double2 z = s[threadIdx.x * T];
         d.red[OFF_DC + 2 * threadIdx.x] = z.x;
@@ -395,7 +411,7 @@ __global__ void k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
         for (int l = 0; l < 3; l++) q[l * T] = u[l];
     }
     __syncthreads();
-    fft_run<true>(s, P, 3 * T, pl, d.tw3);
+    fft_run<true, RS>(s, P, 3 * T, pl, d.tw3);
     for (int idx = threadIdx.x; idx < 3 * T * n3; idx += blockDim.x) {
         const int t = idx % T, r = idx / T, c = r % 3, k3 = r / 3, kx = kx0 + t;
         if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
@@ -403,7 +419,8 @@ __global__ void k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
 }
 
 // ---------------------------------------------------------------- x inverse (C2R)
-__global__ void k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
@@ -425,7 +442,7 @@ __global__ void k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, Xin
         s[x * P + p] = make_double2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    fft_run<true>(s, P, P, pl, d.tw1);
+    fft_run<true, RS>(s, P, P, pl, d.tw1);
     const double invN = 1.0 / (double)N;
     double acc[9];
 #pragma unroll
@@ -469,20 +486,28 @@ __global__ void k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, Xin
         for (int f = 0; f < 9; f++) {
             double x = lane < nw ? sh[f][lane] : 0.0;
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) d.partials[(size_t)blockIdx.x * 9 + f] = x;
+            if (lane == 0) d.partials[(size_t)f * gridDim.x + blockIdx.x] = x;
         }
     }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = (atomicAdd(d.counters + CNT_XINV, 1u) == gridDim.x - 1);
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    __shared__ double fsum[9];
+    if (last) {  // fold the block partials: one warp per field, fixed order
         __threadfence();
+        for (int f = warp; f < 9; f += nw) {
+            double x = 0.0;
+            for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(&d.partials[(size_t)f * gridDim.x + b]);
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) fsum[f] = x;
+        }
+        __syncthreads();
+    }
+    if (last && threadIdx.x == 0) {
         double fl[9], dd[9], du[9];
         for (int f = 0; f < 9; f++) {
-            double x = 0.0;
-            for (unsigned b = 0; b < gridDim.x; b++) x += __ldcg(&d.partials[(size_t)b * 9 + f]);
-            fl[f] = x;
+            fl[f] = fsum[f];
             dd[f] = xp.dvelgradavg[f] - fl[f];
         }
         mm3(dd, xp.dinv, du);
@@ -494,7 +519,8 @@ __global__ void k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, Xin
 // ---------------------------------------------------------------- standalone Green-operator application
 // x passes of evp_green_apply: the 9 real input fields come straight from a
 // caller-owned array tau[c*N + v] and the result goes to out[c*N + v].
-__global__ void k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restrict__ tau) {
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restrict__ tau) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
@@ -510,7 +536,7 @@ __global__ void k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restri
         for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = (row < nrows) ? tau[c * N + v] : 0.0;
     }
     __syncthreads();
-    fft_run<false>(s, P, P, pl, d.tw1);
+    fft_run<false, RS>(s, P, P, pl, d.tw1);
     for (int idx = threadIdx.x; idx < P * n1h; idx += blockDim.x) {
         const int k = idx % n1h, p = idx / n1h;
         const int c = p / G, g = p % G;
@@ -522,7 +548,8 @@ __global__ void k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restri
         if (ra + 1 < nrows) d.spec[((long long)c * nrows + ra + 1) * n1h + k] = make_double2(0.5 * dZ.y, -0.5 * dZ.x);
     }
 }
-__global__ void k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ out) {
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ out) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
@@ -543,7 +570,7 @@ __global__ void k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ o
         s[x * P + p] = make_double2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    fft_run<true>(s, P, P, pl, d.tw1);
+    fft_run<true, RS>(s, P, P, pl, d.tw1);
     const double* sd = reinterpret_cast<const double*>(s);
     for (int idx = threadIdx.x; idx < G * 2 * n1; idx += blockDim.x) {
         const int g = idx / (2 * n1), rem = idx % (2 * n1), half = rem / n1, x = rem % n1;
@@ -556,20 +583,25 @@ __global__ void k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ o
 }
 
 // ---------------------------------------------------------------- launchers
-// A pass needs P * n / (smallest radix) / 4 threads for P pencils of length n
-// (four butterflies per thread).  The FFT kernels carry the butterflies of
-// every radix and use many registers, which caps their block size below 1024:
-// each launcher asks the kernel for its limit and shrinks its tile (pencils
-// per block) until the threads fit.
+// A pass needs P * n / (smallest radix) / (butterflies per thread) threads for
+// P pencils of length n.  Each launcher picks the power-of-two kernels when the
+// plan has only radices 2, 4 and 8, asks the kernel for its block-size limit
+// (set by its register use) and shrinks its tile (pencils per block) until
+// the threads fit.
+static bool plan_pow2(const FftPlan1D& pl) {
+    for (int i = 0; i < pl.nst; i++)
+        if (pl.rad[i] != 2 && pl.rad[i] != 4 && pl.rad[i] != 8) return false;
+    return true;
+}
 static int kernel_max_threads(const void* k) {
     cudaFuncAttributes a{};
     if (cudaFuncGetAttributes(&a, k) != cudaSuccess || a.maxThreadsPerBlock < 32) return 256;
     return a.maxThreadsPerBlock;
 }
 // largest tile T <= T0 whose ncomp * T pencils fit in maxthr threads; thr gets the block size
-static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int want, int maxthr, int& thr) {
+static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int maxb, int want, int maxthr, int& thr) {
     for (int T = T0; T >= 1; T--) {
-        const int need = (ncomp * T * pl.n / min_radix(pl) + 3) / 4;
+        const int need = (ncomp * T * pl.n / min_radix(pl) + maxb - 1) / maxb;
         int t = want > need ? want : need;
         t = (t + 31) / 32 * 32;
         if (t > maxthr) t = maxthr / 32 * 32;
@@ -582,31 +614,40 @@ static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int want, int maxthr
 }
 static int x_rows_per_block(int n1) { return (256 / n1) > 1 ? 256 / n1 : 1; }
 
-void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
-                        double* out, const double* c0, const double* s0, cudaStream_t st) {
-    static const int mx = std::min(kernel_max_threads((const void*)k_green_x_fwd), kernel_max_threads((const void*)k_green_x_inv));
+template <int RS>
+static void green_apply_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
+                           double* out, const double* c0, const double* s0, cudaStream_t st) {
+    static const int mx = std::min(kernel_max_threads((const void*)k_green_x_fwd<RS>), kernel_max_threads((const void*)k_green_x_inv<RS>));
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, 256, mx, thr);
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, fft_maxb<RS>(), 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
-    const int P = 9 * G;
-    const size_t smem = (size_t)P * d.n1 * sizeof(double2);
-    k_green_x_fwd<<<grid, thr, smem, st>>>(d, pl1, G, tau);
+    const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
+    k_green_x_fwd<RS><<<grid, thr, smem, st>>>(d, pl1, G, tau);
     launch_fft_y(d, pl2, 9, false, st);
     launch_fft_z_green(d, pl3, c0, s0, st);
     launch_fft_y(d, pl2, 9, true, st);
-    k_green_x_inv<<<grid, thr, smem, st>>>(d, pl1, G, out);
+    k_green_x_inv<RS><<<grid, thr, smem, st>>>(d, pl1, G, out);
+}
+void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
+                        double* out, const double* c0, const double* s0, cudaStream_t st) {
+    if (plan_pow2(pl1)) green_apply_rs<0>(d, pl1, pl2, pl3, tau, out, c0, s0, st);
+    else green_apply_rs<1>(d, pl1, pl2, pl3, tau, out, c0, s0, st);
 }
 
-void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_x_fwd);
+template <int RS>
+static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
+    static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS>);
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl, 256, mx, thr);
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl, fft_maxb<RS>(), 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
-    const int P = 9 * G;
-    const size_t smem = (size_t)P * d.n1 * sizeof(double2);
-    k_fft_x_fwd<<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
+    const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
+    k_fft_x_fwd<RS><<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
+}
+void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
+    if (plan_pow2(pl)) x_fwd_rs<0>(d, pl, mode, sg_off, st);
+    else x_fwd_rs<1>(d, pl, mode, sg_off, st);
 }
 
 static int y_tile(const Dev& d) {
@@ -615,14 +656,19 @@ static int y_tile(const Dev& d) {
     if (nt < 1) nt = 1;
     return (d.n1h + nt - 1) / nt;
 }
-void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
-    static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true>), kernel_max_threads((const void*)k_fft_y<false>));
+template <int RS>
+static void y_rs(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
+    static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS>), kernel_max_threads((const void*)k_fft_y<false, RS>));
     int thr = 0;
-    const int T = fit_tile(y_tile(d), 1, pl, 128, mx, thr);
+    const int T = fit_tile(y_tile(d), 1, pl, fft_maxb<RS>(), 128, mx, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
     const size_t smem = (size_t)T * d.n2 * sizeof(double2);
-    if (inverse) k_fft_y<true><<<grid, thr, smem, st>>>(d, pl, T);
-    else k_fft_y<false><<<grid, thr, smem, st>>>(d, pl, T);
+    if (inverse) k_fft_y<true, RS><<<grid, thr, smem, st>>>(d, pl, T);
+    else k_fft_y<false, RS><<<grid, thr, smem, st>>>(d, pl, T);
+}
+void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
+    if (plan_pow2(pl)) y_rs<0>(d, pl, ncomp, inverse, st);
+    else y_rs<1>(d, pl, ncomp, inverse, st);
 }
 
 static int z_tile(const Dev& d) {
@@ -631,44 +677,64 @@ static int z_tile(const Dev& d) {
     if (nt < 1) nt = 1;
     return (d.n1h + nt - 1) / nt;
 }
-void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_z_green);
+template <int RS>
+static void z_green_rs(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
+    static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS>);
     int thr = 0;
-    const int T = fit_tile(z_tile(d), 9, pl, 256, mx, thr);
+    const int T = fit_tile(z_tile(d), 9, pl, fft_maxb<RS>(), 256, mx, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
     const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
-    k_fft_z_green<<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
+    k_fft_z_green<RS><<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
+}
+void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
+    if (plan_pow2(pl)) z_green_rs<0>(d, pl, c0, s0, st);
+    else z_green_rs<1>(d, pl, c0, s0, st);
+}
+template <int RS>
+static void z_integ_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
+    static const int mx = kernel_max_threads((const void*)k_fft_z_integ<RS>);
+    int thr = 0;
+    const int T = fit_tile(z_tile(d), 9, pl, fft_maxb<RS>(), 256, mx, thr);
+    dim3 grid((d.n1h + T - 1) / T, d.n2);
+    const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
+    k_fft_z_integ<RS><<<grid, thr, smem, st>>>(d, pl, T, ideriv);
 }
 void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_z_integ);
-    int thr = 0;
-    const int T = fit_tile(z_tile(d), 9, pl, 256, mx, thr);
-    dim3 grid((d.n1h + T - 1) / T, d.n2);
-    const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
-    k_fft_z_integ<<<grid, thr, smem, st>>>(d, pl, T, ideriv);
+    if (plan_pow2(pl)) z_integ_rs<0>(d, pl, ideriv, st);
+    else z_integ_rs<1>(d, pl, ideriv, st);
 }
-void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_x_inv);
+template <int RS>
+static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
+    static const int mx = kernel_max_threads((const void*)k_fft_x_inv<RS>);
     const int ncomp = (mode == 0) ? 9 : 3;
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), ncomp, pl, 256, mx, thr);
+    const int G = fit_tile(x_rows_per_block(d.n1), ncomp, pl, fft_maxb<RS>(), 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
-    const int P = ncomp * G;
-    const size_t smem = (size_t)P * d.n1 * sizeof(double2);
-    k_fft_x_inv<<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
+    const size_t smem = (size_t)ncomp * G * d.n1 * sizeof(double2);
+    k_fft_x_inv<RS><<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
+}
+void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
+    if (plan_pow2(pl)) x_inv_rs<0>(d, pl, mode, p, st);
+    else x_inv_rs<1>(d, pl, mode, p, st);
 }
 
 // Raise the dynamic shared-memory limit of the FFT kernels (once per process).
+template <int RS>
+static void configure_rs() {
+    const int lim = 160 * 1024;
+    cudaFuncSetAttribute(k_fft_x_fwd<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_y<false, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_y<true, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_z_green<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_z_integ<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_x_inv<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_green_x_fwd<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_green_x_inv<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
 void fft_configure() {
-    cudaFuncSetAttribute(k_fft_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_fft_y<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_fft_y<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_fft_z_integ, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_fft_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_green_x_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    cudaFuncSetAttribute(k_green_x_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    configure_rs<0>();
+    configure_rs<1>();
 }
 
 }  // namespace evp

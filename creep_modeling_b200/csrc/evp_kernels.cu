@@ -32,8 +32,25 @@ constexpr int kBlock = 256;
 constexpr int kNewtonBlock = 128;
 
 // ---------------------------------------------------------------- reductions
-// NS sums then NM maxima per thread -> one partial per block -> the last block
-// finishing folds the partials in block order into out[0 .. NS+NM).
+// NS sums then NM maxima per thread -> one partial per block (stored field-major,
+// partials[f * gridDim.x + block]) -> the last block to finish folds them: one
+// warp per field, lane l adding blocks l, l + 32, ... in order, then a fixed
+// shuffle tree, so the result does not depend on timing.
+__device__ __forceinline__ double fold_sum(const double* partials, int nblk, int f, int lane) {
+    double s = 0.0;
+    for (int b = lane; b < nblk; b += 32) s += __ldcg(&partials[(size_t)f * nblk + b]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    return s;  // in lane 0
+}
+__device__ __forceinline__ double fold_max(const double* partials, int nblk, int f, int lane) {
+    double s = -EVP_HUGE;
+    for (int b = lane; b < nblk; b += 32) s = fmax(s, __ldcg(&partials[(size_t)f * nblk + b]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
+    return s;  // in lane 0
+}
+
 template <int NS, int NM>
 __device__ void reduce_store(const double* sums, const double* maxs, double* partials, double* out, unsigned int* counter) {
     constexpr int NF = NS + NM;
@@ -59,7 +76,7 @@ __device__ void reduce_store(const double* sums, const double* maxs, double* par
                 double y = __shfl_down_sync(0xffffffffu, x, o);
                 x = (f < NS) ? x + y : fmax(x, y);
             }
-            if (lane == 0) partials[(size_t)blockIdx.x * NF + f] = x;
+            if (lane == 0) partials[(size_t)f * gridDim.x + blockIdx.x] = x;
         }
     }
     __threadfence();
@@ -68,13 +85,9 @@ __device__ void reduce_store(const double* sums, const double* maxs, double* par
     __syncthreads();
     if (last) {
         __threadfence();
-        for (int f = threadIdx.x; f < NF; f += blockDim.x) {
-            double s = (f < NS) ? 0.0 : -EVP_HUGE;
-            for (unsigned b = 0; b < gridDim.x; b++) {
-                double y = __ldcg(&partials[(size_t)b * NF + f]);
-                s = (f < NS) ? s + y : fmax(s, y);
-            }
-            out[f] = s;
+        for (int f = warp; f < NF; f += nw) {
+            const double x = (f < NS) ? fold_sum(partials, gridDim.x, f, lane) : fold_max(partials, gridDim.x, f, lane);
+            if (lane == 0) out[f] = x;
         }
         if (threadIdx.x == 0) *counter = 0;
     }
@@ -1761,20 +1774,26 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
         for (int f = 0; f < 9; f++) {
             double x = lane < nw ? sh[f][lane] : 0.0;
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) d.partials[(size_t)blockIdx.x * 9 + f] = x;
+            if (lane == 0) d.partials[(size_t)f * gridDim.x + blockIdx.x] = x;
         }
     }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = (atomicAdd(d.counters + CNT_UPD2, 1u) == gridDim.x - 1);
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    __shared__ double fsum[9];
+    if (last) {
         __threadfence();
+        for (int f = warp; f < 9; f += nw) {
+            const double x = fold_sum(d.partials, gridDim.x, f, lane);
+            if (lane == 0) fsum[f] = x;
+        }
+        __syncthreads();
+    }
+    if (last && threadIdx.x == 0) {
         double va[9], fc[9], di[9], dd[9], du[9];
         for (int f = 0; f < 9; f++) {
-            double x = 0.0;
-            for (unsigned b = 0; b < gridDim.x; b++) x += __ldcg(&d.partials[(size_t)b * 9 + f]);
-            va[f] = x;
+            va[f] = fsum[f];
             fc[f] = __ldcg(&d.red[OFF_UPD1 + 9 + f]) / dav;
         }
         if (inv3u(fc, di) != 0) set_err(d.err, 1);
