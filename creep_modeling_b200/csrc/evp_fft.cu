@@ -614,6 +614,43 @@ static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int maxb, int want, 
 }
 static int x_rows_per_block(int n1) { return (256 / n1) > 1 ? 256 / n1 : 1; }
 
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n < 1) n = 1;
+    }
+    return n;
+}
+// Tile choice: among tiles T <= T0 that fit (fit_tile), take the one with the
+// least (waves of blocks) x (T + 1): block time grows with T, and a last wave
+// that is mostly empty costs as much as a full one.
+template <class BlocksOf, class SmemOf>
+static int choose_tile(const void* kern, int T0, int ncomp, const FftPlan1D& pl, int maxb, int want, int maxthr, BlocksOf blocks_of,
+                       SmemOf smem_of, int& thr) {
+    int best = -1, best_thr = 0;
+    double best_cost = 0.0;
+    for (int T = T0; T >= 1; T--) {
+        int t = 0;
+        if (fit_tile(T, ncomp, pl, maxb, want, maxthr, t) != T) continue;
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, t, smem_of(T)) != cudaSuccess || per_sm < 1) continue;
+        const long long slots = (long long)per_sm * sm_count();
+        const long long waves = (blocks_of(T) + slots - 1) / slots;
+        const double cost = (double)waves * (T + 1);
+        if (best < 0 || cost < best_cost) {
+            best = T;
+            best_cost = cost;
+            best_thr = t;
+        }
+    }
+    if (best < 0) return fit_tile(T0, ncomp, pl, maxb, want, maxthr, thr);
+    thr = best_thr;
+    return best;
+}
+
 template <int RS>
 static void green_apply_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
                            double* out, const double* c0, const double* s0, cudaStream_t st) {
@@ -639,7 +676,10 @@ template <int RS>
 static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
     static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS>);
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl, fft_maxb<RS>(), 256, mx, thr);
+    const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
+    const int G = choose_tile((const void*)k_fft_x_fwd<RS>, x_rows_per_block(d.n1), 9, pl, fft_maxb<RS>(), 128, mx,
+                              [&](int g) { return (npr + g - 1) / g; },
+                              [&](int g) { return (size_t)9 * g * d.n1 * sizeof(double2); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
@@ -660,7 +700,9 @@ template <int RS>
 static void y_rs(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
     static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS>), kernel_max_threads((const void*)k_fft_y<false, RS>));
     int thr = 0;
-    const int T = fit_tile(y_tile(d), 1, pl, fft_maxb<RS>(), 128, mx, thr);
+    const int T = choose_tile((const void*)k_fft_y<false, RS>, y_tile(d), 1, pl, fft_maxb<RS>(), 64, mx,
+                              [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n3 * ncomp; },
+                              [&](int t) { return (size_t)t * d.n2 * sizeof(double2); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
     const size_t smem = (size_t)T * d.n2 * sizeof(double2);
     if (inverse) k_fft_y<true, RS><<<grid, thr, smem, st>>>(d, pl, T);
@@ -681,7 +723,9 @@ template <int RS>
 static void z_green_rs(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS>);
     int thr = 0;
-    const int T = fit_tile(z_tile(d), 9, pl, fft_maxb<RS>(), 256, mx, thr);
+    const int T = choose_tile((const void*)k_fft_z_green<RS>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+                              [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
+                              [&](int t) { return (size_t)9 * t * d.n3 * sizeof(double2); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
     const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
     k_fft_z_green<RS><<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
@@ -694,7 +738,9 @@ template <int RS>
 static void z_integ_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_integ<RS>);
     int thr = 0;
-    const int T = fit_tile(z_tile(d), 9, pl, fft_maxb<RS>(), 256, mx, thr);
+    const int T = choose_tile((const void*)k_fft_z_integ<RS>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+                              [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
+                              [&](int t) { return (size_t)9 * t * d.n3 * sizeof(double2); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
     const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
     k_fft_z_integ<RS><<<grid, thr, smem, st>>>(d, pl, T, ideriv);
@@ -708,7 +754,10 @@ static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvPara
     static const int mx = kernel_max_threads((const void*)k_fft_x_inv<RS>);
     const int ncomp = (mode == 0) ? 9 : 3;
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), ncomp, pl, fft_maxb<RS>(), 256, mx, thr);
+    const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
+    const int G = choose_tile((const void*)k_fft_x_inv<RS>, x_rows_per_block(d.n1), ncomp, pl, fft_maxb<RS>(), 128, mx,
+                              [&](int g) { return (npr + g - 1) / g; },
+                              [&](int g) { return (size_t)ncomp * g * d.n1 * sizeof(double2); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const size_t smem = (size_t)ncomp * G * d.n1 * sizeof(double2);

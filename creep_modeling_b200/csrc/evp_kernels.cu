@@ -345,7 +345,7 @@ void launch_gas_compl(const Dev& d, double tdot, double complgas, int modal, cud
 
 // ---------------------------------------------------------------- k_corr
 // velgrad += (dvelgradref + du) F^{-1}; averages; dL statistics; mixing.
-__global__ void __launch_bounds__(kBlock) k_corr(Dev d, CorrParams p) {
+__global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) {
     const long long N = d.N;
     __shared__ double du[9];
     if (threadIdx.x < 9) du[threadIdx.x] = __ldcg(&d.red[OFF_DU + threadIdx.x]);
@@ -387,7 +387,12 @@ __global__ void __launch_bounds__(kBlock) k_corr(Dev d, CorrParams p) {
     }
     reduce_store<31, 0>(s, nullptr, d.partials, d.red + OFF_CORR, d.counters + CNT_CORR);
 }
-void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st) { k_corr<<<d.grid, kBlock, 0, st>>>(d, p); }
+// fewer blocks than the other voxel kernels: each thread handles several voxels, which spreads the
+// 31-field block reduction over more loads
+void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st) {
+    const int grid = d.grid < 148 * 2 ? d.grid : 148 * 2;
+    k_corr<<<grid, kBlock, 0, st>>>(d, p);
+}
 
 // ---------------------------------------------------------------- local constitutive solve
 // plastic_strain_rate (various_functions.f90:1367-1419) + elastic_strain_rate (1422-1436)
