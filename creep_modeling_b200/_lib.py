@@ -12,6 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_build" / "libevp_b200.so"
 EXPORTED = (
     "evp_solve_file", "evp_open", "evp_advance", "evp_get_field", "evp_last_rows", "evp_stats", "evp_close",
     "evp_kernel_times", "evp_green_apply", "evp_green_apply_noalloc", "evp_last_error", "evp_version",
+    "evp_server_open", "evp_submit", "evp_poll", "evp_wait", "evp_server_close",
 )
 
 STATUS = {
@@ -40,6 +41,25 @@ class Report(ctypes.Structure):
         ("n3", ctypes.c_int),
         ("h2d_bytes", ctypes.c_longlong),
         ("d2h_bytes", ctypes.c_longlong),
+    ]
+
+
+class Status(ctypes.Structure):
+    """evp_status: the state of one served request."""
+
+    _fields_ = [
+        ("state", ctypes.c_int),
+        ("status", ctypes.c_int),
+        ("macrosteps", ctypes.c_int),
+        ("n1", ctypes.c_int),
+        ("n2", ctypes.c_int),
+        ("n3", ctypes.c_int),
+        ("voxel_iters", ctypes.c_longlong),
+        ("queued_s", ctypes.c_double),
+        ("run_s", ctypes.c_double),
+        ("latency_s", ctypes.c_double),
+        ("footprint_bytes", ctypes.c_ulonglong),
+        ("error", ctypes.c_char * 256),
     ]
 
 
@@ -84,6 +104,18 @@ def load(path: Path | str | None = None):
     L.evp_last_error.restype = ctypes.c_char_p
     L.evp_version.argtypes = []
     L.evp_version.restype = ctypes.c_int
+    u64 = ctypes.c_ulonglong
+    L.evp_server_open.argtypes = [u64, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(vp)]
+    L.evp_server_open.restype = ctypes.c_int
+    L.evp_submit.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                             ctypes.POINTER(u64)]
+    L.evp_submit.restype = ctypes.c_int
+    L.evp_poll.argtypes = [vp, u64, ctypes.POINTER(Status)]
+    L.evp_poll.restype = ctypes.c_int
+    L.evp_wait.argtypes = [vp, u64, ctypes.c_double, ctypes.POINTER(Status)]
+    L.evp_wait.restype = ctypes.c_int
+    L.evp_server_close.argtypes = [vp]
+    L.evp_server_close.restype = ctypes.c_int
     _lib = L
     return L
 

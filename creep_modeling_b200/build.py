@@ -19,7 +19,7 @@ OUT = PKG / "_build"
 LIB = OUT / "libevp_b200.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["evp_solver.cu", "evp_kernels.cu", "evp_fft.cu", "evp_green.cu", "evp_deck.cpp"]
+SOURCES = ["evp_solver.cu", "evp_kernels.cu", "evp_fft.cu", "evp_green.cu", "evp_deck.cpp", "evp_server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", f"-I{INCLUDE}"]
 

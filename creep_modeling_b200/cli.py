@@ -5,10 +5,13 @@
 Unknown flags print the reference's message and stop.  Exit status: 0 on
 success, 1 on a solver error (the reference's ``stop 1`` paths); a deck error
 also exits 1 here, where the Fortran ``stop 'msg'`` exits 0 (callers treat
-both through the missing/short results.csv path).
+both through the missing/short results.csv path).  With ``EVP_SERVER_SOCKET``
+naming a running ``python -m creep_modeling_b200.serve`` socket, the solve is
+submitted there instead of running in this process.
 """
 from __future__ import annotations
 
+import os
 import sys
 
 
@@ -51,6 +54,16 @@ def main(argv=None) -> int:
     from . import solver
     from ._lib import EvpError
 
+    sock = os.environ.get("EVP_SERVER_SOCKET")
+    if sock and os.path.exists(sock):  # serving mode: the resident server runs the solve
+        from .serve import submit_via_socket
+
+        st = submit_via_socket(sock, opts["in"], opts["out"], opts["mix"], opts["modal"])
+        if st.get("status", -7) != 0:
+            print(f"\n[{st.get('status')}] {st.get('error', '')}", file=sys.stderr)
+            return 1
+        print(f"\nMACROSTEPS={st['macrosteps']} VOXEL_ITERS={st['voxel_iters']} LATENCY={st['latency_s']:.3f}s (served)")
+        return 0
     try:
         rep = solver.run_solver(opts["in"], opts["out"], opts["nthreads"], opts["fftw_save"], opts["mix"], opts["modal"])
     except EvpError as e:

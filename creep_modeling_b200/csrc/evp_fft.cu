@@ -615,13 +615,12 @@ static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int maxb, int want, 
 static int x_rows_per_block(int n1) { return (256 / n1) > 1 ? 256 / n1 : 1; }
 
 static int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
+    static const int n = [] {
+        int dev = 0, c = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n < 1) n = 1;
-    }
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        return c < 1 ? 1 : c;
+    }();
     return n;
 }
 // Tile choice: among tiles T <= T0 that fit (fit_tile), take the one with the

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
@@ -126,12 +127,13 @@ public:
     T* dalloc(size_t n) {
         void* p = nullptr;
         if (n == 0) return nullptr;
-        CK(cudaMalloc(&p, n * sizeof(T)));
+        CK(cudaMallocAsync(&p, n * sizeof(T), st));  // stream-ordered: no device-wide sync, so concurrent solves do not stall
         allocs.push_back(p);
         return (T*)p;
     }
     ~Solver() {
-        for (void* p : allocs) cudaFree(p);
+        for (void* p : allocs) cudaFreeAsync(p, st);
+        if (st) cudaStreamSynchronize(st);
         if (h_red) cudaFreeHost(h_red);
         if (h_err) cudaFreeHost(h_err);
         if (ev0) cudaEventDestroy(ev0);
@@ -223,8 +225,8 @@ public:
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
-        static bool configured = false;
-        if (!configured) { fft_configure(); configured = true; }
+        static std::once_flag configured;
+        std::call_once(configured, [] { fft_configure(); });
         allocate();
         upload_and_init();
         modal = (modal_flag != 0);

@@ -103,6 +103,51 @@ int evp_green_apply(const double* d_tau, double* d_out, int n1, int n2, int n3, 
 int evp_green_apply_noalloc(const double* d_tau, double* d_out, int n1, int n2, int n3, const double* c0,
                             const double* s0, void* stream);
 
+/* ---- Serving: a resident request loop (the reference has no counterpart; it
+ * runs one solver process per request, utils/run.py:169-196, and calibrate.py
+ * runs two or three such processes at once, calibrate.py:1053-1057).
+ *
+ * A server keeps every admitted solve's fields on the device until the solve
+ * ends and writes the same files as evp_solve_file.  Requests wait in arrival
+ * order; a request is admitted as soon as fewer than max_inflight solves run
+ * and its estimated device footprint fits the budget beside the running ones
+ * (a later, smaller request may go first when the oldest one does not fit).
+ * Admitted solves run concurrently, each on its own CUDA stream and host
+ * thread, so the kernels of solves of different grid sizes overlap on the GPU
+ * and one solve's host work hides behind another's device work.  A solve's
+ * results do not depend on what else runs beside it. */
+typedef struct evp_server evp_server;
+
+typedef struct evp_status {
+    int state;             /* 0 queued, 1 running, 2 done */
+    int status;            /* when done: 0 or a status code as evp_solve_file returns */
+    int macrosteps;        /* macrosteps completed */
+    int n1, n2, n3;        /* grid */
+    long long voxel_iters; /* voxels x equilibrium iterations executed */
+    double queued_s;       /* submit -> admission */
+    double run_s;          /* admission -> files written */
+    double latency_s;      /* submit -> files written */
+    unsigned long long footprint_bytes; /* device-memory estimate used for admission */
+    char error[256];       /* message when status != 0 */
+} evp_status;
+
+/* hbm_budget_bytes: device memory the running solves may hold together (0: 85 % of
+ * the free memory at open).  max_inflight: solves run at once (<= 0: 16).
+ * tune_cache: reserved for a tile-shape cache; may be NULL. */
+int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const char* tune_cache, evp_server** out);
+/* Queue one solve (same deck and flags as evp_solve_file; precision 0 = plain FP64).
+ * flags: EVP_WRITE_FILES (results, diagnostics and VTK, as the executable) or
+ * EVP_WRITE_CSV (results and diagnostics only).  The ticket identifies it. */
+int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision, int flags,
+               unsigned long long* ticket);
+/* Current state of a request (non-blocking). */
+int evp_poll(evp_server* srv, unsigned long long ticket, evp_status* st);
+/* Block until the request is done or timeout_s passes (timeout_s < 0: no limit);
+ * returns 0 when done, 1 on timeout. */
+int evp_wait(evp_server* srv, unsigned long long ticket, double timeout_s, evp_status* st);
+/* Let queued and running solves finish, then release the server. */
+int evp_server_close(evp_server* srv);
+
 /* Message of the last failing call on this thread. */
 const char* evp_last_error(void);
 int evp_version(void);
