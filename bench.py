@@ -9,7 +9,9 @@ reference's (unshipped) microstructures.  A "step" is one macrostep
 (increment): every equilibrium iteration it needs plus the large-strain
 updates.  Metric: voxel-iters/s = voxels x equilibrium iterations / device
 seconds (CUDA events on the solver's stream, max over ranks).  The state
-(~1.8 kB/voxel, 460 MB) is larger than the 126 MB L2, so no flush is needed.
+(~2 kB/voxel, 0.5 GB) is larger than the 126 MB L2, so no flush is needed.
+The line's "serving" object times a bounded sample of the served request stream
+(see serving_sample).
 
 --gpus N > 1 runs N independent replicas (the solve does not shard), one
 process per GPU, and sums their voxel-iters.
@@ -186,6 +188,45 @@ def run_reference(args, ws, rank):
     return 0
 
 
+def serving_sample(k: int, scale: float, rate: float) -> dict:
+    """The served request stream, bounded: the first k requests of the seeded stream (grid
+    edges 16-96, Arrhenius-scaled gamma0 at 475/525/575, creep 80-220 MPa) with their
+    increment counts scaled by `scale`, submitted to one resident server at their Poisson
+    arrival times (rate per s).  Latency = submit -> results.csv and diagnostics.csv written."""
+    import numpy as np
+
+    from creep_modeling_b200 import decks
+    from creep_modeling_b200.serve import Server
+
+    td = Path(tempfile.mkdtemp(prefix="evp_serve_"))
+    cases = [decks.case_c5(i, scale) for i in range(k)]
+    ffts = [decks.write_case(c, td / f"r{i}") for i, c in enumerate(cases)]  # untimed
+    arr = decks.stream_arrivals(k, rate)
+    with Server(0, 16) as srv:
+        t0 = time.perf_counter()
+        tickets = []
+        for i, f in enumerate(ffts):
+            dt = arr[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(srv.submit(f, td / f"o{i}", mix=1, modal=0, csv_only=True))
+        sts = [srv.wait(t) for t in tickets]
+        span = time.perf_counter() - t0
+    ok = [s for s in sts if s["status"] == 0]
+    lat = np.array([s["latency_s"] for s in ok])
+    return {
+        "requests": k, "completed": len(ok),
+        "failed": [{"request": i, "status": s["status"], "error": s["error"][:120]} for i, s in enumerate(sts) if s["status"] != 0],
+        "arrival_rate_per_s": rate, "increments_scale": scale,
+        "edges": [c.n for c in cases], "increments": [c.processes[0].nsteps for c in cases],
+        "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+        "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+        "solves_per_hour": len(ok) / span * 3600.0, "voxel_iters_per_s": sum(s["voxel_iters"] for s in ok) / span,
+        "span_s": span, "max_inflight": 16, "precision": "plain FP64 (error vs the FP64 path: 0 by construction)",
+        "sample": f"first {k} requests of the seeded stream, increments x{scale}, arrivals Poisson {rate}/s",
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +238,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds of CPU time for --impl reference")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the served-stream sample (0: skip)")
+    ap.add_argument("--serve-scale", type=float, default=0.1, help="increment-count scale of the served-stream sample")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
@@ -320,6 +363,13 @@ def main(argv=None) -> int:
         except Exception as exc:  # pragma: no cover
             cpu = {"value": None, "error": str(exc)}
 
+    serving = None
+    if args.serve_requests > 0:
+        try:
+            serving = serving_sample(args.serve_requests, args.serve_scale, 20.0)
+        except Exception as exc:  # pragma: no cover - reported, not hidden
+            serving = {"error": str(exc)}
+
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": gpu_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -328,6 +378,7 @@ def main(argv=None) -> int:
                                "(plain FP64)", "voxels": n ** 3, "equilibrium_iters": int(iters),
                    "parallelism": f"replicas x{ws}", "l2": "state (~460 MB) larger than L2; no flush"},
         "wall_s": wall, "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
     if pg:

@@ -78,6 +78,31 @@ class Loading:
     ictrl: int = -1
 
 
+def _nearest_seed(pts: np.ndarray, seeds: np.ndarray, box: np.ndarray) -> np.ndarray:
+    """1-based index of the nearest seed under the minimum-image (periodic) distance; exact
+    ties go to the lowest seed index."""
+    try:
+        from scipy.spatial import cKDTree
+    except ImportError:  # pragma: no cover - scipy is part of the environment
+        cKDTree = None
+    if cKDTree is not None and len(seeds) > 1:
+        tree = cKDTree(np.mod(seeds, box), boxsize=box)
+        dist, idx = tree.query(pts, k=2)
+        tie = dist[:, 0] == dist[:, 1]
+        best = np.where(tie, np.minimum(idx[:, 0], idx[:, 1]), idx[:, 0])
+        return best.astype(np.int64) + 1
+    best = np.full(pts.shape[0], np.inf)
+    grain = np.zeros(pts.shape[0], dtype=np.int64)
+    for g in range(len(seeds)):
+        d = pts - seeds[g]
+        d -= box * np.round(d / box)
+        r2 = np.einsum("ij,ij->i", d, d)
+        m = r2 < best
+        best[m] = r2[m]
+        grain[m] = g + 1
+    return grain
+
+
 def voronoi_micro(n: int | tuple[int, int, int], ngrains: int, seed: int, phase2_spheres: float = 0.0,
                   sphere_r: tuple[float, float] = (2.0, 4.0)):
     """Return (grain[n1,n2,n3], phase[...], euler[ngrains,3] in degrees).
@@ -93,16 +118,7 @@ def voronoi_micro(n: int | tuple[int, int, int], ngrains: int, seed: int, phase2
     ii, jj, kk = np.meshgrid(np.arange(n1) + 0.5, np.arange(n2) + 0.5, np.arange(n3) + 0.5, indexing="ij")
     pts = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1)
     box = np.array([n1, n2, n3], dtype=float)
-    best = np.full(pts.shape[0], np.inf)
-    grain = np.zeros(pts.shape[0], dtype=np.int64)
-    for g in range(ngrains):
-        d = pts - seeds[g]
-        d -= box * np.round(d / box)
-        r2 = np.einsum("ij,ij->i", d, d)
-        m = r2 < best
-        best[m] = r2[m]
-        grain[m] = g + 1
-    grain = grain.reshape(n1, n2, n3)
+    grain = _nearest_seed(pts, seeds, box).reshape(n1, n2, n3)
     phase = np.ones((n1, n2, n3), dtype=np.int64)
     if phase2_spheres > 0.0:
         target = phase2_spheres * n1 * n2 * n3
@@ -290,3 +306,49 @@ def write_case(case: Case, root: Path, micro_cache: dict | None = None) -> Path:
     fft = root / "fft.in"
     write_fft_in(fft, case.n, micro, root / "cupl2.sx", root / "cuel.sx", case.processes, phase2=phase2)
     return fft
+
+
+def case_c4(i: int, nsteps: int = 150) -> Case:
+    """Solve i of the batched calibration sweep (seed 1000 + i): grid edge from {16, 32, 48, 64},
+    32-500 grains, tau0 log-uniform in [50, 200] MPa, n uniform in [5, 20], theta0 log-uniform in
+    [100, 1000] MPa (theta1 = 20 <= theta0, as the reference requires); creep at 120 MPa."""
+    rng = np.random.default_rng(1000 + i)
+    n = int(rng.choice([16, 32, 48, 64]))
+    ngr = int(rng.integers(32, 501))
+    tau0 = float(math.exp(rng.uniform(math.log(50.0), math.log(200.0))))
+    nrs = float(rng.uniform(5.0, 20.0))
+    thet0 = float(math.exp(rng.uniform(math.log(100.0), math.log(1000.0))))
+    mat = Material(nrs=nrs, tau0f=tau0, tau0b=tau0, thet0=thet0)
+    return Case(f"sweep{i}", n, ngr, 1000 + i, mat,
+                [Loading(kind="creep", stress33=120.0, udot33=1e-4, tdot=10.0, nsteps=nsteps, error=1e-5, erroral=1e-9,
+                         itmax=200)])
+
+
+ARRHENIUS_Q = 250e3  # J/mol
+GAS_R = 8.314462618  # J/(mol K)
+
+
+def case_c5(i: int, increments_scale: float = 1.0) -> Case:
+    """Request i of the served stream (seed stream 5): grid edge exp(U[ln 16, ln 96]) rounded to a
+    multiple of 8; temperature from {475, 525, 575} (taken as kelvin: the reference has no
+    temperature model) scaling gamma0 = 1e-3 exp(-Q/R (1/T - 1/525)) with Q = 250 kJ/mol; creep
+    stress U[80, 220] MPa; U{50..400} increments (times increments_scale, at least 1); 32-500 grains,
+    at most one per 8 voxels."""
+    rng = np.random.default_rng([5, i])
+    edge = int(round(math.exp(rng.uniform(math.log(16.0), math.log(96.0))) / 8.0) * 8)
+    edge = min(max(edge, 16), 96)
+    temp = float(rng.choice([475.0, 525.0, 575.0]))
+    gamd0 = 1e-3 * math.exp(-ARRHENIUS_Q / GAS_R * (1.0 / temp - 1.0 / 525.0))
+    stress = float(rng.uniform(80.0, 220.0))
+    nsteps = max(1, int(round(int(rng.integers(50, 401)) * increments_scale)))
+    ngr = min(int(rng.integers(32, 501)), edge ** 3 // 8)
+    mat = Material(nrs=10.0, gamd0=gamd0)
+    return Case(f"stream{i}_T{int(temp)}", edge, ngr, 5000 + i, mat,
+                [Loading(kind="creep", stress33=stress, udot33=1e-4, tdot=10.0, nsteps=nsteps, error=1e-5, erroral=1e-9,
+                         itmax=200)])
+
+
+def stream_arrivals(k: int, rate_per_s: float = 20.0, seed: int = 5) -> np.ndarray:
+    """Arrival times (s) of the first k requests of a Poisson stream."""
+    rng = np.random.default_rng([seed, 99])
+    return np.cumsum(rng.exponential(1.0 / rate_per_s, size=k))
