@@ -75,6 +75,7 @@ struct Dev {
     // spectrum, twiddles, grid-update scratch
     double2 *spec;
     double2 *tw1, *tw2, *tw3;
+    float2 *tw1f, *tw2f, *tw3f;  // FP32 twiddles of the mixed-precision path (may be null)
     double *dv3, *xnode;
     // reductions
     double *partials, *red;
@@ -128,15 +129,16 @@ void launch_cell2node(const Dev& d, double tdot, int ideriv, cudaStream_t st);
 
 // FFT engine (evp_fft.cu)
 FftPlan1D make_plan(int n);
-void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st);
+// prec 1: the equilibrium chain's spectrum, FFTs and Green operator in FP32 (mixed precision)
+void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st, int prec = 0);
 void fft_configure();
 // Green operator applied to 9 real fields tau -> out (caller-owned device arrays);
 // d supplies the grid, spectrum scratch, twiddles and error word.
 void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
                         double* out, const double* c0, const double* s0, cudaStream_t st);
-void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st);
-void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st);
+void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st, int prec = 0);
+void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st, int prec = 0);
 void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st);
-void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st);
+void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st, int prec = 0);
 
 }  // namespace evp

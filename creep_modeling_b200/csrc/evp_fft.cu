@@ -25,49 +25,72 @@
 
 namespace evp {
 
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// Complex arithmetic on double2 (FP64 path) and float2 (FP32 spectrum of the mixed-precision path).
+template <class CT>
+struct CxT;
+template <>
+struct CxT<double2> {
+    using T = double;
+};
+template <>
+struct CxT<float2> {
+    using T = float;
+};
+template <class CT>
+__device__ __forceinline__ CT mk(typename CxT<CT>::T x, typename CxT<CT>::T y) {
+    CT r;
+    r.x = x;
+    r.y = y;
+    return r;
+}
+template <class CT>
+__device__ __forceinline__ CT cadd(CT a, CT b) { return mk<CT>(a.x + b.x, a.y + b.y); }
+template <class CT>
+__device__ __forceinline__ CT csub(CT a, CT b) { return mk<CT>(a.x - b.x, a.y - b.y); }
+template <class CT>
+__device__ __forceinline__ CT cmul(CT a, CT b) { return mk<CT>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <class CT>
+__device__ __forceinline__ CT cconj(CT a) { return mk<CT>(a.x, -a.y); }
 // multiply by -i (forward) or +i (inverse)
-template <bool INV>
-__device__ __forceinline__ double2 mul_mi(double2 a) { return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
+template <bool INV, class CT>
+__device__ __forceinline__ CT mul_mi(CT a) { return INV ? mk<CT>(-a.y, a.x) : mk<CT>(a.y, -a.x); }
 
-template <int R, bool INV>
-__device__ __forceinline__ void dft_small(double2 (&v)[R], const double2* __restrict__ tw, int n) {
+template <int R, bool INV, class CT>
+__device__ __forceinline__ void dft_small(CT (&v)[R], const CT* __restrict__ tw, int n) {
+    using T = typename CxT<CT>::T;
     if constexpr (R == 2) {
-        double2 a = v[0], b = v[1];
+        CT a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     } else if constexpr (R == 4) {
-        double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]), t3 = mul_mi<INV>(csub(v[1], v[3]));
+        CT t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]), t3 = mul_mi<INV, CT>(csub(v[1], v[3]));
         v[0] = cadd(t0, t2);
         v[2] = csub(t0, t2);
         v[1] = cadd(t1, t3);
         v[3] = csub(t1, t3);
     } else if constexpr (R == 8) {
-        const double c = 0.70710678118654752440;
-        double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
-        dft_small<4, INV>(e, tw, n);
-        dft_small<4, INV>(o, tw, n);
-        double2 w1 = INV ? make_double2(c, c) : make_double2(c, -c);
-        double2 w3 = INV ? make_double2(-c, c) : make_double2(-c, -c);
-        double2 p0 = o[0], p1 = cmul(o[1], w1), p2 = mul_mi<INV>(o[2]), p3 = cmul(o[3], w3);
+        const T c = (T)0.70710678118654752440;
+        CT e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<4, INV, CT>(e, tw, n);
+        dft_small<4, INV, CT>(o, tw, n);
+        CT w1 = INV ? mk<CT>(c, c) : mk<CT>(c, -c);
+        CT w3 = INV ? mk<CT>(-c, c) : mk<CT>(-c, -c);
+        CT p0 = o[0], p1 = cmul(o[1], w1), p2 = mul_mi<INV, CT>(o[2]), p3 = cmul(o[3], w3);
         v[0] = cadd(e[0], p0); v[4] = csub(e[0], p0);
         v[1] = cadd(e[1], p1); v[5] = csub(e[1], p1);
         v[2] = cadd(e[2], p2); v[6] = csub(e[2], p2);
         v[3] = cadd(e[3], p3); v[7] = csub(e[3], p3);
     } else {
-        double2 in[R];
+        CT in[R];
 #pragma unroll
         for (int r = 0; r < R; r++) in[r] = v[r];
         const int step = n / R;
 #pragma unroll
         for (int q = 0; q < R; q++) {
-            double2 acc = in[0];
+            CT acc = in[0];
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                double2 w = tw[((r * q) % R) * step];
+                CT w = tw[((r * q) % R) * step];
                 if (INV) w.y = -w.y;
                 acc = cadd(acc, cmul(in[r], w));
             }
@@ -78,10 +101,10 @@ __device__ __forceinline__ void dft_small(double2 (&v)[R], const double2* __rest
 
 // One Stockham stage over P pencils of length n stored element-major in
 // shared memory: element e of pencil p at s[e*ES + p].
-template <int R, bool INV, int MAXB>
-__device__ __forceinline__ void fft_stage(double2* s, int ES, int P, int n, int Ns, const double2* __restrict__ tw) {
+template <int R, bool INV, int MAXB, class CT>
+__device__ __forceinline__ void fft_stage(CT* s, int ES, int P, int n, int Ns, const CT* __restrict__ tw) {
     const int nb = n / R, total = nb * P;
-    double2 v[MAXB][R];
+    CT v[MAXB][R];
 #pragma unroll
     for (int q = 0; q < MAXB; q++) {
         const int b = threadIdx.x + q * blockDim.x;
@@ -100,11 +123,11 @@ __device__ __forceinline__ void fft_stage(double2* s, int ES, int P, int n, int 
             const int step = jm * (n / (Ns * R));
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                double2 w = tw[r * step];
+                CT w = tw[r * step];
                 if (INV) w.y = -w.y;
                 v[q][r] = cmul(v[q][r], w);
             }
-            dft_small<R, INV>(v[q], tw, n);
+            dft_small<R, INV, CT>(v[q], tw, n);
             const int idxD = (j / Ns) * Ns * R + jm;
 #pragma unroll
             for (int r = 0; r < R; r++) s[(idxD + r * Ns) * ES + p] = v[q][r];
@@ -120,24 +143,24 @@ __device__ __forceinline__ void fft_stage(double2* s, int ES, int P, int n, int 
 template <int RS>
 __host__ __device__ constexpr int fft_maxb() { return RS == 0 ? 2 : 4; }
 
-template <bool INV, int RS>
-__device__ void fft_run(double2* s, int ES, int P, const FftPlan1D& pl, const double2* __restrict__ tw) {
+template <bool INV, int RS, class CT>
+__device__ void fft_run(CT* s, int ES, int P, const FftPlan1D& pl, const CT* __restrict__ tw) {
     constexpr int MB = fft_maxb<RS>();
     int Ns = 1;
     for (int st = 0; st < pl.nst; st++) {
         const int R = pl.rad[st];
         switch (R) {
-            case 2: fft_stage<2, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
-            case 4: fft_stage<4, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
-            case 8: fft_stage<8, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+            case 2: fft_stage<2, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+            case 4: fft_stage<4, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+            case 8: fft_stage<8, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
             default:
                 if constexpr (RS != 0) {
                     switch (R) {
-                        case 3: fft_stage<3, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
-                        case 5: fft_stage<5, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
-                        case 7: fft_stage<7, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
-                        case 11: fft_stage<11, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
-                        case 13: fft_stage<13, INV, MB>(s, ES, P, pl.n, Ns, tw); break;
+                        case 3: fft_stage<3, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+                        case 5: fft_stage<5, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+                        case 7: fft_stage<7, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+                        case 11: fft_stage<11, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+                        case 13: fft_stage<13, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
                         default: break;
                     }
                 }
@@ -179,11 +202,26 @@ static int min_radix(const FftPlan1D& pl) {
     return pl.nst ? r : 1;
 }
 
+// twiddle table of an axis in the complex type of the pass
+template <class CT>
+__device__ __forceinline__ const CT* twid(const Dev& d, int axis);
+template <>
+__device__ __forceinline__ const double2* twid<double2>(const Dev& d, int axis) {
+    return axis == 1 ? d.tw1 : (axis == 2 ? d.tw2 : d.tw3);
+}
+template <>
+__device__ __forceinline__ const float2* twid<float2>(const Dev& d, int axis) {
+    return axis == 1 ? d.tw1f : (axis == 2 ? d.tw2f : d.tw3f);
+}
+
 // ---------------------------------------------------------------- x forward (R2C)
 // mode 0: P'_ij = J * ((sigma - <sigma>) F^{-T})_ij ; mode 1: (L F)_ij (grid update)
-template <int RS>
+template <int RS, class CT>
 __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
-    extern __shared__ double2 s[];
+    using Re = typename CxT<CT>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT* const s = reinterpret_cast<CT*>(smem_raw);
+    CT* const spec = reinterpret_cast<CT*>(d.spec);
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
     const int nrows = d.n2 * d.n3;
@@ -219,40 +257,41 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_fwd(Dev d, FftPl
 #pragma unroll
             for (int c = 0; c < 9; c++) val[c] = 0.0;
         }
-        double* sd = reinterpret_cast<double*>(s);
+        Re* sd = reinterpret_cast<Re*>(s);
 #pragma unroll
-        for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = val[c];
+        for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = (Re)val[c];
     }
     __syncthreads();
-    fft_run<false, RS>(s, P, P, pl, d.tw1);
+    fft_run<false, RS, CT>(s, P, P, pl, twid<CT>(d, 1));
     // unpack the two real rows of every pencil
     for (int idx = threadIdx.x; idx < P * n1h; idx += blockDim.x) {
         const int k = idx % n1h, p = idx / n1h;
         const int c = p / G, g = p % G;
-        const double2 Z = s[k * P + p];
-        const double2 Zc = cconj(s[((n1 - k) % n1) * P + p]);
-        const double2 Xa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
-        const double2 dZ = csub(Z, Zc);
-        const double2 Xb = make_double2(0.5 * dZ.y, -0.5 * dZ.x);
+        const CT Z = s[k * P + p];
+        const CT Zc = cconj(s[((n1 - k) % n1) * P + p]);
+        const CT Xa = mk<CT>((Re)0.5 * (Z.x + Zc.x), (Re)0.5 * (Z.y + Zc.y));
+        const CT dZ = csub(Z, Zc);
+        const CT Xb = mk<CT>((Re)0.5 * dZ.y, (Re)-0.5 * dZ.x);
         const int ra = 2 * (pair0 + g);
-        if (ra < nrows) d.spec[((long long)c * nrows + ra) * n1h + k] = Xa;
-        if (ra + 1 < nrows) d.spec[((long long)c * nrows + ra + 1) * n1h + k] = Xb;
+        if (ra < nrows) spec[((long long)c * nrows + ra) * n1h + k] = Xa;
+        if (ra + 1 < nrows) spec[((long long)c * nrows + ra + 1) * n1h + k] = Xb;
     }
 }
 
 // ---------------------------------------------------------------- y (C2C)
-template <bool INV, int RS>
+template <bool INV, int RS, class CT>
 __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_y(Dev d, FftPlan1D pl, int T) {
-    extern __shared__ double2 s[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT* const s = reinterpret_cast<CT*>(smem_raw);
     const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
     const int kx0 = blockIdx.x * T, k3 = blockIdx.y, c = blockIdx.z;
-    double2* base = d.spec + ((long long)c * n3 + k3) * n2 * n1h;
+    CT* base = reinterpret_cast<CT*>(d.spec) + ((long long)c * n3 + k3) * n2 * n1h;
     for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
         const int t = idx % T, j = idx / T, kx = kx0 + t;
-        s[j * T + t] = (kx < n1h) ? base[(long long)j * n1h + kx] : make_double2(0.0, 0.0);
+        s[j * T + t] = (kx < n1h) ? base[(long long)j * n1h + kx] : mk<CT>(0, 0);
     }
     __syncthreads();
-    fft_run<INV, RS>(s, T, T, pl, d.tw2);
+    fft_run<INV, RS, CT>(s, T, T, pl, twid<CT>(d, 2));
     for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
         const int t = idx % T, j = idx / T, kx = kx0 + t;
         if (kx < n1h) base[(long long)j * n1h + kx] = s[j * T + t];
@@ -265,74 +304,97 @@ __device__ __forceinline__ double xi_of(int k, int n) {
     return (k + 1 <= n / 2) ? twopi * (double)k / (double)n : twopi * (double)(k - n) / (double)n;
 }
 
-template <int RS>
+// 3x3 inverse for the Green step: the FP64 path uses the LU inverse of the other
+// kernels; the FP32 path the adjugate over the determinant (singular: returns 1).
+__device__ __forceinline__ int inv3_any(const double* a, double* ai) { return inv3u(a, ai); }
+__device__ __forceinline__ int inv3_any(const float* a, float* ai) {
+    const float c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const float det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (det == 0.0f) return 1;
+    const float r = 1.0f / det;
+    ai[0] = c00 * r;
+    ai[1] = (a[2] * a[7] - a[1] * a[8]) * r;
+    ai[2] = (a[1] * a[5] - a[2] * a[4]) * r;
+    ai[3] = c01 * r;
+    ai[4] = (a[0] * a[8] - a[2] * a[6]) * r;
+    ai[5] = (a[2] * a[3] - a[0] * a[5]) * r;
+    ai[6] = c02 * r;
+    ai[7] = (a[1] * a[6] - a[0] * a[7]) * r;
+    ai[8] = (a[0] * a[4] - a[1] * a[3]) * r;
+    return 0;
+}
+
+template <int RS, class CT>
 __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
-    extern __shared__ double2 s[];
-    __shared__ double c0[81], s0[81];
+    using Re = typename CxT<CT>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT* const s = reinterpret_cast<CT*>(smem_raw);
+    CT* const spec = reinterpret_cast<CT*>(d.spec);
+    __shared__ Re c0[81], s0[81];
     const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
     const int kx0 = blockIdx.x * T, j = blockIdx.y;
     const int P = 9 * T;
-    for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = c0g[i]; s0[i] = s0g[i]; }
+    for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = (Re)c0g[i]; s0[i] = (Re)s0g[i]; }
     const long long plane = (long long)n2 * n1h;
     for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
         const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
-        s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
+        s[k3 * P + c * T + t] = (kx < n1h) ? spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : mk<CT>(0, 0);
     }
     __syncthreads();
-    fft_run<false, RS>(s, P, P, pl, d.tw3);
+    fft_run<false, RS, CT>(s, P, P, pl, twid<CT>(d, 3));
     const bool nyq_y = (n2 % 2 == 0 && j == n2 / 2);
-    const double xiy = xi_of(j, n2);
+    const Re xiy = (Re)xi_of(j, n2);
     for (int idx = threadIdx.x; idx < T * n3; idx += blockDim.x) {
         const int t = idx % T, k3 = idx / T, kx = kx0 + t;
         if (kx >= n1h) continue;
-        double2* q = s + k3 * P + t;
-        double2 a[9], r[9];
+        CT* q = s + k3 * P + t;
+        CT a[9], r[9];
 #pragma unroll
         for (int c = 0; c < 9; c++) a[c] = q[c * T];
         const bool nyq = (n1 % 2 == 0 && kx == n1 / 2) || nyq_y || (n3 % 2 == 0 && k3 == n3 / 2 && n3 > 1);
         if (kx == 0 && j == 0 && k3 == 0) {
 #pragma unroll
-            for (int c = 0; c < 9; c++) r[c] = make_double2(0.0, 0.0);
+            for (int c = 0; c < 9; c++) r[c] = mk<CT>(0, 0);
         } else if (nyq) {
             // Nyquist planes: Gamma = -s0 (various_functions.f90:646-651)
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                double2 acc = make_double2(0.0, 0.0);
+                CT acc = mk<CT>(0, 0);
 #pragma unroll
                 for (int e = 0; e < 9; e++) {
-                    const double g = -s0[c * 9 + e];
+                    const Re g = -s0[c * 9 + e];
                     acc.x += g * a[e].x;
                     acc.y += g * a[e].y;
                 }
                 r[c] = acc;
             }
         } else {
-            const double xi[3] = {xi_of(kx, n1), xiy, (n3 == 1) ? 0.0 : xi_of(k3, n3)};
-            double A[9], ai[9];
+            const Re xi[3] = {(Re)xi_of(kx, n1), xiy, (n3 == 1) ? (Re)0 : (Re)xi_of(k3, n3)};
+            Re A[9], ai[9];
 #pragma unroll
             for (int i = 0; i < 3; i++)
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    double x = 0.0;
+                    Re x = 0;
 #pragma unroll
                     for (int jj = 0; jj < 3; jj++)
 #pragma unroll
                         for (int l = 0; l < 3; l++) x += c0[((i * 3 + jj) * 3 + k) * 3 + l] * (xi[jj] * xi[l]);
                     A[3 * i + k] = x;
                 }
-            if (inv3u(A, ai) != 0) atomicOr(d.err, 1);
+            if (inv3_any(A, ai) != 0) atomicOr(d.err, 1);
             // r_ij = -xi_j * sum_k ai_ik (P xi)_k
-            double2 pv[3], wv[3];
+            CT pv[3], wv[3];
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-                double2 acc = make_double2(0.0, 0.0);
+                CT acc = mk<CT>(0, 0);
 #pragma unroll
                 for (int l = 0; l < 3; l++) { acc.x += a[3 * k + l].x * xi[l]; acc.y += a[3 * k + l].y * xi[l]; }
                 pv[k] = acc;
             }
 #pragma unroll
             for (int i = 0; i < 3; i++) {
-                double2 acc = make_double2(0.0, 0.0);
+                CT acc = mk<CT>(0, 0);
 #pragma unroll
                 for (int k = 0; k < 3; k++) { acc.x += ai[3 * i + k] * pv[k].x; acc.y += ai[3 * i + k] * pv[k].y; }
                 wv[i] = acc;
@@ -340,16 +402,16 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_green(Dev d, Fft
 #pragma unroll
             for (int i = 0; i < 3; i++)
 #pragma unroll
-                for (int jj = 0; jj < 3; jj++) r[3 * i + jj] = make_double2(-xi[jj] * wv[i].x, -xi[jj] * wv[i].y);
+                for (int jj = 0; jj < 3; jj++) r[3 * i + jj] = mk<CT>(-xi[jj] * wv[i].x, -xi[jj] * wv[i].y);
         }
 #pragma unroll
         for (int c = 0; c < 9; c++) q[c * T] = r[c];
     }
     __syncthreads();
-    fft_run<true, RS>(s, P, P, pl, d.tw3);
+    fft_run<true, RS, CT>(s, P, P, pl, twid<CT>(d, 3));
     for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
         const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
-        if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
+        if (kx < n1h) spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
     }
 }
 
@@ -366,7 +428,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
         s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    fft_run<false, RS>(s, P, P, pl, d.tw3);
+    fft_run<false, RS, double2>(s, P, P, pl, d.tw3);
     if (blockIdx.x == 0 && j == 0 && threadIdx.x < 9) {
         const double2 z = s[threadIdx.x * T];
         d.red[OFF_DC + 2 * threadIdx.x] = z.x;
@@ -411,7 +473,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
         for (int l = 0; l < 3; l++) q[l * T] = u[l];
     }
     __syncthreads();
-    fft_run<true, RS>(s, P, 3 * T, pl, d.tw3);
+    fft_run<true, RS, double2>(s, P, 3 * T, pl, d.tw3);
     for (int idx = threadIdx.x; idx < 3 * T * n3; idx += blockDim.x) {
         const int t = idx % T, r = idx / T, c = r % 3, k3 = r / 3, kx = kx0 + t;
         if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
@@ -419,9 +481,12 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
 }
 
 // ---------------------------------------------------------------- x inverse (C2R)
-template <int RS>
+template <int RS, class CT>
 __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
-    extern __shared__ double2 s[];
+    using Re = typename CxT<CT>::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT* const s = reinterpret_cast<CT*>(smem_raw);
+    const CT* const spec = reinterpret_cast<const CT*>(d.spec);
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
     const int nrows = d.n2 * d.n3;
@@ -434,15 +499,15 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPl
         const int ra = 2 * (pair0 + g);
         const int k = (x <= n1 / 2) ? x : n1 - x;
         const bool cj = (x > n1 / 2);
-        double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
-        if (ra < nrows) A = d.spec[((long long)c * nrows + ra) * n1h + k];
-        if (ra + 1 < nrows) B = d.spec[((long long)c * nrows + ra + 1) * n1h + k];
-        if (k == 0 || (even && k == n1 / 2)) { A.y = 0.0; B.y = 0.0; }
+        CT A = mk<CT>(0, 0), B = mk<CT>(0, 0);
+        if (ra < nrows) A = spec[((long long)c * nrows + ra) * n1h + k];
+        if (ra + 1 < nrows) B = spec[((long long)c * nrows + ra + 1) * n1h + k];
+        if (k == 0 || (even && k == n1 / 2)) { A.y = 0; B.y = 0; }
         if (cj) { A.y = -A.y; B.y = -B.y; }
-        s[x * P + p] = make_double2(A.x - B.y, A.y + B.x);
+        s[x * P + p] = mk<CT>(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    fft_run<true, RS>(s, P, P, pl, d.tw1);
+    fft_run<true, RS, CT>(s, P, P, pl, twid<CT>(d, 1));
     const double invN = 1.0 / (double)N;
     double acc[9];
 #pragma unroll
@@ -452,12 +517,12 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPl
         const int row = 2 * (pair0 + g) + half;
         if (row >= nrows) continue;
         const long long v = (long long)row * n1 + x;
-        const double* sd = reinterpret_cast<const double*>(s);
+        const Re* sd = reinterpret_cast<const Re*>(s);
         if (mode == 0) {
             double t[9], fi[9], u[9];
 #pragma unroll
             for (int c = 0; c < 9; c++) {
-                t[c] = sd[2 * (x * P + c * G + g) + half] / (double)N;
+                t[c] = (double)sd[2 * (x * P + c * G + g) + half] / (double)N;
                 d.dvr[c * N + v] = t[c];
                 fi[c] = d.Finv[c * N + v];
             }
@@ -466,7 +531,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPl
 #pragma unroll
             for (int c = 0; c < 9; c++) acc[c] += w * u[c];
         } else {
-            for (int c = 0; c < ncomp; c++) d.dv3[c * N + v] = sd[2 * (x * P + c * G + g) + half] / (double)N;
+            for (int c = 0; c < ncomp; c++) d.dv3[c * N + v] = (double)sd[2 * (x * P + c * G + g) + half] / (double)N;
         }
     }
     (void)invN;
@@ -536,7 +601,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_fwd(Dev d, Fft
         for (int c = 0; c < 9; c++) sd[2 * (x * P + c * G + g) + half] = (row < nrows) ? tau[c * N + v] : 0.0;
     }
     __syncthreads();
-    fft_run<false, RS>(s, P, P, pl, d.tw1);
+    fft_run<false, RS, double2>(s, P, P, pl, d.tw1);
     for (int idx = threadIdx.x; idx < P * n1h; idx += blockDim.x) {
         const int k = idx % n1h, p = idx / n1h;
         const int c = p / G, g = p % G;
@@ -570,7 +635,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_inv(Dev d, Fft
         s[x * P + p] = make_double2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    fft_run<true, RS>(s, P, P, pl, d.tw1);
+    fft_run<true, RS, double2>(s, P, P, pl, d.tw1);
     const double* sd = reinterpret_cast<const double*>(s);
     for (int idx = threadIdx.x; idx < G * 2 * n1; idx += blockDim.x) {
         const int g = idx / (2 * n1), rem = idx % (2 * n1), half = rem / n1, x = rem % n1;
@@ -660,9 +725,9 @@ static void green_apply_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& 
     const int grid = (npairs + G - 1) / G;
     const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
     k_green_x_fwd<RS><<<grid, thr, smem, st>>>(d, pl1, G, tau);
-    launch_fft_y(d, pl2, 9, false, st);
-    launch_fft_z_green(d, pl3, c0, s0, st);
-    launch_fft_y(d, pl2, 9, true, st);
+    launch_fft_y(d, pl2, 9, false, st, 0);
+    launch_fft_z_green(d, pl3, c0, s0, st, 0);
+    launch_fft_y(d, pl2, 9, true, st, 0);
     k_green_x_inv<RS><<<grid, thr, smem, st>>>(d, pl1, G, out);
 }
 void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* tau,
@@ -671,22 +736,23 @@ void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
     else green_apply_rs<1>(d, pl1, pl2, pl3, tau, out, c0, s0, st);
 }
 
-template <int RS>
+template <int RS, class CT>
 static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS>);
+    static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS, CT>);
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
-    const int G = choose_tile((const void*)k_fft_x_fwd<RS>, x_rows_per_block(d.n1), 9, pl, fft_maxb<RS>(), 128, mx,
+    const int G = choose_tile((const void*)k_fft_x_fwd<RS, CT>, x_rows_per_block(d.n1), 9, pl, fft_maxb<RS>(), 128, mx,
                               [&](int g) { return (npr + g - 1) / g; },
-                              [&](int g) { return (size_t)9 * g * d.n1 * sizeof(double2); }, thr);
+                              [&](int g) { return (size_t)9 * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
-    const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
-    k_fft_x_fwd<RS><<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
+    const size_t smem = (size_t)9 * G * d.n1 * sizeof(CT);
+    k_fft_x_fwd<RS, CT><<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
 }
-void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
-    if (plan_pow2(pl)) x_fwd_rs<0>(d, pl, mode, sg_off, st);
-    else x_fwd_rs<1>(d, pl, mode, sg_off, st);
+void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st, int prec) {
+    const bool f32 = prec != 0 && mode == 0;  // the grid-update chain (mode 1) stays FP64
+    if (plan_pow2(pl)) f32 ? x_fwd_rs<0, float2>(d, pl, mode, sg_off, st) : x_fwd_rs<0, double2>(d, pl, mode, sg_off, st);
+    else f32 ? x_fwd_rs<1, float2>(d, pl, mode, sg_off, st) : x_fwd_rs<1, double2>(d, pl, mode, sg_off, st);
 }
 
 static int y_tile(const Dev& d) {
@@ -695,21 +761,21 @@ static int y_tile(const Dev& d) {
     if (nt < 1) nt = 1;
     return (d.n1h + nt - 1) / nt;
 }
-template <int RS>
+template <int RS, class CT>
 static void y_rs(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
-    static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS>), kernel_max_threads((const void*)k_fft_y<false, RS>));
+    static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS, CT>), kernel_max_threads((const void*)k_fft_y<false, RS, CT>));
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_y<false, RS>, y_tile(d), 1, pl, fft_maxb<RS>(), 64, mx,
+    const int T = choose_tile((const void*)k_fft_y<false, RS, CT>, y_tile(d), 1, pl, fft_maxb<RS>(), 64, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n3 * ncomp; },
-                              [&](int t) { return (size_t)t * d.n2 * sizeof(double2); }, thr);
+                              [&](int t) { return (size_t)t * d.n2 * sizeof(CT); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
-    const size_t smem = (size_t)T * d.n2 * sizeof(double2);
-    if (inverse) k_fft_y<true, RS><<<grid, thr, smem, st>>>(d, pl, T);
-    else k_fft_y<false, RS><<<grid, thr, smem, st>>>(d, pl, T);
+    const size_t smem = (size_t)T * d.n2 * sizeof(CT);
+    if (inverse) k_fft_y<true, RS, CT><<<grid, thr, smem, st>>>(d, pl, T);
+    else k_fft_y<false, RS, CT><<<grid, thr, smem, st>>>(d, pl, T);
 }
-void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
-    if (plan_pow2(pl)) y_rs<0>(d, pl, ncomp, inverse, st);
-    else y_rs<1>(d, pl, ncomp, inverse, st);
+void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st, int prec) {
+    if (plan_pow2(pl)) prec ? y_rs<0, float2>(d, pl, ncomp, inverse, st) : y_rs<0, double2>(d, pl, ncomp, inverse, st);
+    else prec ? y_rs<1, float2>(d, pl, ncomp, inverse, st) : y_rs<1, double2>(d, pl, ncomp, inverse, st);
 }
 
 static int z_tile(const Dev& d) {
@@ -718,20 +784,20 @@ static int z_tile(const Dev& d) {
     if (nt < 1) nt = 1;
     return (d.n1h + nt - 1) / nt;
 }
-template <int RS>
+template <int RS, class CT>
 static void z_green_rs(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS>);
+    static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS, CT>);
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_z_green<RS>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+    const int T = choose_tile((const void*)k_fft_z_green<RS, CT>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
-                              [&](int t) { return (size_t)9 * t * d.n3 * sizeof(double2); }, thr);
+                              [&](int t) { return (size_t)9 * t * d.n3 * sizeof(CT); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
-    const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
-    k_fft_z_green<RS><<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
+    const size_t smem = (size_t)9 * T * d.n3 * sizeof(CT);
+    k_fft_z_green<RS, CT><<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
 }
-void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
-    if (plan_pow2(pl)) z_green_rs<0>(d, pl, c0, s0, st);
-    else z_green_rs<1>(d, pl, c0, s0, st);
+void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st, int prec) {
+    if (plan_pow2(pl)) prec ? z_green_rs<0, float2>(d, pl, c0, s0, st) : z_green_rs<0, double2>(d, pl, c0, s0, st);
+    else prec ? z_green_rs<1, float2>(d, pl, c0, s0, st) : z_green_rs<1, double2>(d, pl, c0, s0, st);
 }
 template <int RS>
 static void z_integ_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
@@ -748,35 +814,42 @@ void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStrea
     if (plan_pow2(pl)) z_integ_rs<0>(d, pl, ideriv, st);
     else z_integ_rs<1>(d, pl, ideriv, st);
 }
-template <int RS>
+template <int RS, class CT>
 static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
-    static const int mx = kernel_max_threads((const void*)k_fft_x_inv<RS>);
+    static const int mx = kernel_max_threads((const void*)k_fft_x_inv<RS, CT>);
     const int ncomp = (mode == 0) ? 9 : 3;
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
-    const int G = choose_tile((const void*)k_fft_x_inv<RS>, x_rows_per_block(d.n1), ncomp, pl, fft_maxb<RS>(), 128, mx,
+    const int G = choose_tile((const void*)k_fft_x_inv<RS, CT>, x_rows_per_block(d.n1), ncomp, pl, fft_maxb<RS>(), 128, mx,
                               [&](int g) { return (npr + g - 1) / g; },
-                              [&](int g) { return (size_t)ncomp * g * d.n1 * sizeof(double2); }, thr);
+                              [&](int g) { return (size_t)ncomp * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
-    const size_t smem = (size_t)ncomp * G * d.n1 * sizeof(double2);
-    k_fft_x_inv<RS><<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
+    const size_t smem = (size_t)ncomp * G * d.n1 * sizeof(CT);
+    k_fft_x_inv<RS, CT><<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
 }
-void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
-    if (plan_pow2(pl)) x_inv_rs<0>(d, pl, mode, p, st);
-    else x_inv_rs<1>(d, pl, mode, p, st);
+void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st, int prec) {
+    const bool f32 = prec != 0 && mode == 0;  // the grid-update chain (mode 1) stays FP64
+    if (plan_pow2(pl)) f32 ? x_inv_rs<0, float2>(d, pl, mode, p, st) : x_inv_rs<0, double2>(d, pl, mode, p, st);
+    else f32 ? x_inv_rs<1, float2>(d, pl, mode, p, st) : x_inv_rs<1, double2>(d, pl, mode, p, st);
 }
 
 // Raise the dynamic shared-memory limit of the FFT kernels (once per process).
+template <int RS, class CT>
+static void configure_ct() {
+    const int lim = 160 * 1024;
+    cudaFuncSetAttribute(k_fft_x_fwd<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_y<false, RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_y<true, RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_z_green<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(k_fft_x_inv<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
 template <int RS>
 static void configure_rs() {
     const int lim = 160 * 1024;
-    cudaFuncSetAttribute(k_fft_x_fwd<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(k_fft_y<false, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(k_fft_y<true, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(k_fft_z_green<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    configure_ct<RS, double2>();
+    configure_ct<RS, float2>();
     cudaFuncSetAttribute(k_fft_z_integ<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(k_fft_x_inv<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(k_green_x_fwd<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(k_green_x_inv<RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }

@@ -217,7 +217,7 @@ int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const
 int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision, int flags,
                unsigned long long* ticket) {
     if (!srv || !fft_in || !ticket) return srv_fail("evp_submit: null argument", -7);
-    if (precision != 0) return srv_fail("evp_submit: only precision 0 (plain FP64) is built", -2);
+    if (precision != 0 && precision != 1) return srv_fail("evp_submit: precision must be 0 (plain FP64) or 1 (mixed)", -7);
     if ((flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) == 0) return srv_fail("evp_submit: flags must ask for EVP_WRITE_FILES or EVP_WRITE_CSV", -7);
     Request r;
     r.fft = fft_in;
@@ -225,7 +225,7 @@ int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix
     r.mix = mix;
     r.modal = modal;
     r.precision = precision;
-    r.flags = flags & (EVP_WRITE_FILES | EVP_WRITE_CSV | EVP_VERBOSE);
+    r.flags = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV | EVP_VERBOSE)) | (precision == 1 ? EVP_MIXED : 0);
     if (!deck_grid(r.fft, r.n1, r.n2, r.n3)) return srv_fail("evp_submit: cannot read the grid size from " + r.fft, -1);
     r.foot = footprint(r.n1, r.n2, r.n3);
     r.t_submit = Clock::now();

@@ -144,6 +144,7 @@ public:
     // ---- host<->device byte counters and the optional per-kernel event timer
     long long h2d = 0, d2h = 0;
     bool profile = false, write_vtk_files = false;
+    int prec = 0;  // 1: mixed precision (FP32 spectrum, FFTs and Green operator in the equilibrium chain)
     struct KTime {
         std::string name;
         long long n = 0;
@@ -205,6 +206,7 @@ public:
         write_files = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) != 0;
         write_vtk_files = (flags & EVP_WRITE_FILES) != 0;
         profile = (flags & EVP_PROFILE) != 0;
+        prec = (flags & EVP_MIXED) ? 1 : 0;
         verbose = (flags & EVP_VERBOSE) != 0;
         outdir = out.empty() ? std::string("evpfft_outputs/") : out;
         if (write_files) {
@@ -308,6 +310,18 @@ public:
             sync();
         };
         twiddles(dk.n1, d.tw1); twiddles(dk.n2, d.tw2); twiddles(dk.n3, d.tw3);
+        if (prec) {  // FP32 copies, rounded from the same long-double angles
+            auto twiddles_f = [&](int n, float2* dst) {
+                std::vector<float2> t(n);
+                for (int e = 0; e < n; e++) {
+                    long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)n;
+                    t[e] = make_float2((float)cosl(ang), (float)sinl(ang));
+                }
+                h2d_copy(dst, t.data(), n * sizeof(float2));
+            };
+            d.tw1f = dalloc<float2>(dk.n1); d.tw2f = dalloc<float2>(dk.n2); d.tw3f = dalloc<float2>(dk.n3);
+            twiddles_f(dk.n1, d.tw1f); twiddles_f(dk.n2, d.tw2f); twiddles_f(dk.n3, d.tw3f);
+        }
         // phases
         std::vector<PhaseDev> ph(dk.nph);
         for (int p = 0; p < dk.nph; p++) {
@@ -508,14 +522,14 @@ public:
     void equilibrium_iteration(bool fresh_sgavg) {
         ProcessData& p = P();
         if (fresh_sgavg) K("k_sgavg", [&] { launch_sgavg(d, st); });
-        K("k_fft_x_fwd", [&] { launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st); });
-        K("k_fft_y_fwd", [&] { launch_fft_y(d, pl2, 9, false, st); });
-        K("k_fft_z_green", [&] { launch_fft_z_green(d, pl3, d_c0, d_s0, st); });
-        K("k_fft_y_inv", [&] { launch_fft_y(d, pl2, 9, true, st); });
+        K("k_fft_x_fwd", [&] { launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st, prec); });
+        K("k_fft_y_fwd", [&] { launch_fft_y(d, pl2, 9, false, st, prec); });
+        K("k_fft_z_green", [&] { launch_fft_z_green(d, pl3, d_c0, d_s0, st, prec); });
+        K("k_fft_y_inv", [&] { launch_fft_y(d, pl2, 9, true, st, prec); });
         XinvParams xp;
         std::memcpy(xp.dvelgradavg, dvelgradavg, sizeof(xp.dvelgradavg));
         if (inv3(dinvc, xp.dinv) != 0) throw SolveError("Singular matrix in lu_inverse (correction_to_current)", -3);
-        K("k_fft_x_inv", [&] { launch_fft_x_inv(d, pl1, 0, xp, st); });
+        K("k_fft_x_inv", [&] { launch_fft_x_inv(d, pl1, 0, xp, st, prec); });
         CorrParams cp;
         cp.mix = mix;
         cp.Lscale = std::max(lvmavg, EVP_TINY);

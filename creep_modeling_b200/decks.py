@@ -122,12 +122,22 @@ def voronoi_micro(n: int | tuple[int, int, int], ngrains: int, seed: int, phase2
     phase = np.ones((n1, n2, n3), dtype=np.int64)
     if phase2_spheres > 0.0:
         target = phase2_spheres * n1 * n2 * n3
-        while (phase == 2).sum() < target:
+        count = 0
+        while count < target:
             c = rng.uniform(0.0, 1.0, 3) * box
             r = rng.uniform(*sphere_r)
-            d = np.stack([ii - c[0], jj - c[1], kk - c[2]], axis=-1)
+            # voxel centres within the sphere's bounding box, wrapped periodically (same test as over the whole grid)
+            lo = np.floor(c - r - 0.5).astype(int)
+            hi = np.ceil(c + r - 0.5).astype(int)
+            ax = [np.arange(lo[a], hi[a] + 1) for a in range(3)]
+            gi, gj, gk = np.meshgrid(*ax, indexing="ij")
+            d = np.stack([gi + 0.5 - c[0], gj + 0.5 - c[1], gk + 0.5 - c[2]], axis=-1)
             d -= box * np.round(d / box)
-            phase[np.einsum("...i,...i->...", d, d) <= r * r] = 2
+            inside = np.einsum("...i,...i->...", d, d) <= r * r
+            wi, wj, wk = gi[inside] % n1, gj[inside] % n2, gk[inside] % n3
+            fresh = phase[wi, wj, wk] != 2
+            count += np.unique((wi[fresh] * n2 + wj[fresh]) * n3 + wk[fresh]).size  # voxels newly in phase 2
+            phase[wi, wj, wk] = 2
     return grain, phase, euler
 
 

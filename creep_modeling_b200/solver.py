@@ -31,6 +31,7 @@ WRITE_FILES = 1
 VERBOSE = 2
 WRITE_CSV = 4
 PROFILE = 8
+MIXED = 16
 
 
 def run_solver(fft_in, out_dir="evpfft_outputs/", nthreads=0, fftw_save="", mix=1, modal=1) -> _lib.Report:
@@ -49,11 +50,13 @@ class Solve:
     """A device-resident solve advanced macrostep by macrostep."""
 
     def __init__(self, fft_in, out_dir="", mix=1, modal=1, write_files=False, verbose=False, csv_only=False,
-                 profile=False):
+                 profile=False, precision=0):
+        """precision 0: plain FP64; 1: mixed (FP32 spectrum, FFTs and Green operator in the
+        equilibrium iteration; FP64 local Newton, reductions and F/rotation updates)."""
         L = _lib.load()
         h = ctypes.c_void_p()
         flags = ((WRITE_FILES if write_files else 0) | (VERBOSE if verbose else 0) | (WRITE_CSV if csv_only else 0)
-                 | (PROFILE if profile else 0))
+                 | (PROFILE if profile else 0) | (MIXED if precision else 0))
         _lib.check(L.evp_open(str(fft_in).encode(), str(out_dir).encode(), int(mix), int(modal), flags, ctypes.byref(h)))
         self._h = h
         rep = self.stats()

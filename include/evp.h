@@ -42,6 +42,8 @@ typedef struct evp_report {
 #define EVP_VERBOSE 2      /* print the progress line (various_functions.f90:2693-2743) */
 #define EVP_WRITE_CSV 4    /* write results.csv and diagnostics.csv only (no VTK) */
 #define EVP_PROFILE 8      /* time every kernel launch with CUDA events (evp_kernel_times) */
+#define EVP_MIXED 16       /* mixed precision: the equilibrium iteration's spectrum, FFTs and Green-operator
+                              application in FP32; local Newton, reductions and F/rotation updates in FP64 */
 
 /* Whole solve with the executable's semantics: replaces one
  * `LS-EVPFFT --in fft_in --out out_dir --mix mix --modal modal` process
@@ -135,7 +137,8 @@ typedef struct evp_status {
  * the free memory at open).  max_inflight: solves run at once (<= 0: 16).
  * tune_cache: reserved for a tile-shape cache; may be NULL. */
 int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const char* tune_cache, evp_server** out);
-/* Queue one solve (same deck and flags as evp_solve_file; precision 0 = plain FP64).
+/* Queue one solve (same deck and flags as evp_solve_file; precision 0 = plain FP64,
+ * 1 = mixed precision as EVP_MIXED).
  * flags: EVP_WRITE_FILES (results, diagnostics and VTK, as the executable) or
  * EVP_WRITE_CSV (results and diagnostics only).  The ticket identifies it. */
 int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision, int flags,
