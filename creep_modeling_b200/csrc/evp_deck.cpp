@@ -4,16 +4,62 @@
 #include "evp_deck.h"
 #include "evp_math.cuh"
 
+#include <algorithm>
+#include <atomic>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <thread>
 #include <unistd.h>
 
 namespace evp {
 namespace {
+
+// One microstructure record "phi1 Phi phi2 i j k grain phase" with blanks, tabs or
+// commas between values: the common form without Fortran 'd' exponents.
+bool micro_fast(const char* p, const char* e, double* e3, long* i5) {
+    auto skip = [&]() {
+        while (p < e && (*p == ' ' || *p == '\t' || *p == ',')) p++;
+        if (p < e && *p == '+') p++;
+    };
+    for (int k = 0; k < 3; k++) {
+        skip();
+        auto r = std::from_chars(p, e, e3[k]);
+        if (r.ec != std::errc() || (r.ptr < e && (*r.ptr == 'd' || *r.ptr == 'D'))) return false;
+        p = r.ptr;
+    }
+    for (int k = 0; k < 5; k++) {
+        skip();
+        auto r = std::from_chars(p, e, i5[k]);
+        if (r.ec != std::errc()) return false;
+        p = r.ptr;
+    }
+    return true;
+}
+// The same record read the general way ('d' exponents allowed).
+bool micro_slow(const char* p, const char* e, double* e3, long* i5) {
+    std::string rec(p, e - p);
+    for (char& c : rec)
+        if (c == ',' || c == '\t') c = ' ';
+        else if (c == 'd' || c == 'D') c = 'e';
+    const char* s = rec.c_str();
+    char* q = nullptr;
+    for (int k = 0; k < 3; k++) {
+        e3[k] = std::strtod(s, &q);
+        if (q == s) return false;
+        s = q;
+    }
+    for (int k = 0; k < 5; k++) {
+        i5[k] = std::strtol(s, &q, 10);
+        if (q == s) return false;
+        s = q;
+    }
+    return true;
+}
 
 // A file as a list of records; list-directed reads consume whole records.
 class Records {
@@ -86,28 +132,39 @@ public:
     }
     std::vector<double> reals(size_t n) { auto t = tokens(n); std::vector<double> v; for (auto& s : t) v.push_back(real(s)); return v; }
     std::vector<long> ints(size_t n) { auto t = tokens(n); std::vector<long> v; for (auto& s : t) v.push_back(integer(s)); return v; }
-    // fast path for microstructure records: 3 reals + 5 integers
-    void micro_record(double* e3, long* i5) {
-        check();
-        const char* p = buf_.data() + starts_[pos_];
-        const char* end = buf_.data() + ends_[pos_];
-        pos_++;
-        std::string rec(p, end - p);
-        for (char& c : rec)
-            if (c == ',' || c == '\t') c = ' ';
-            else if (c == 'd' || c == 'D') c = 'e';
-        const char* s = rec.c_str();
-        char* q = nullptr;
-        for (int k = 0; k < 3; k++) {
-            e3[k] = std::strtod(s, &q);
-            if (q == s) throw DeckError("short microstructure record in '" + path_ + "'", -1);
-            s = q;
+    // microstructure records (3 reals + 5 integers per line), records pos_ .. pos_ + n - 1,
+    // parsed on several host threads into e3[3n], i5[5n]
+    void micro_records(size_t n, double* e3, long* i5) {
+        if (pos_ + n > starts_.size()) throw DeckError("unexpected end of file in '" + path_ + "'", -1);
+        const size_t first = pos_;
+        unsigned nt = std::thread::hardware_concurrency();
+        nt = nt < 1 ? 1 : (nt > 16 ? 16 : nt);
+        if (n < 4096) nt = 1;
+        std::atomic<long long> bad{-1};
+        auto work = [&](size_t a, size_t b) {
+            for (size_t k = a; k < b; k++) {
+                const char* p = buf_.data() + starts_[first + k];
+                const char* e = buf_.data() + ends_[first + k];
+                if (!micro_fast(p, e, e3 + 3 * k, i5 + 5 * k) && !micro_slow(p, e, e3 + 3 * k, i5 + 5 * k)) {
+                    long long expect = -1;
+                    bad.compare_exchange_strong(expect, (long long)k);
+                    return;
+                }
+            }
+        };
+        if (nt == 1) {
+            work(0, n);
+        } else {
+            std::vector<std::thread> th;
+            const size_t chunk = (n + nt - 1) / nt;
+            for (unsigned t = 0; t < nt; t++) {
+                const size_t a = t * chunk, b = std::min(n, a + chunk);
+                if (a < b) th.emplace_back(work, a, b);
+            }
+            for (auto& t : th) t.join();
         }
-        for (int k = 0; k < 5; k++) {
-            i5[k] = std::strtol(s, &q, 10);
-            if (q == s) throw DeckError("short microstructure record in '" + path_ + "'", -1);
-            s = q;
-        }
+        if (bad.load() >= 0) throw DeckError("short microstructure record in '" + path_ + "'", -1);
+        pos_ += n;
     }
 
 private:
@@ -279,10 +336,12 @@ Deck parse_deck(const std::string& fft_in) {
     d.phase_id.assign(N, 0);
     {
         Records m(filetext);
-        for (long long kkk = 0; kkk < N; kkk++) {
-            double e3[3];
-            long i5[5];
-            m.micro_record(e3, i5);
+        std::vector<double> E3(3 * (size_t)N);
+        std::vector<long> I5(5 * (size_t)N);
+        m.micro_records((size_t)N, E3.data(), I5.data());
+        for (long long kkk = 0; kkk < N; kkk++) {  // in file order: a later record for a voxel wins
+            const double* e3 = &E3[3 * kkk];
+            const long* i5 = &I5[5 * kkk];
             long ii = i5[0], jj = i5[1], kk = i5[2];
             if (ii < 1 || ii > d.n1 || jj < 1 || jj > d.n2 || kk < 1 || kk > d.n3)
                 throw DeckError("voxel index out of range in microstructure file", -1);
