@@ -1430,6 +1430,8 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                     for (int q = 0; q < 6; q++) gall[6 * k + q] = t6[q];
                 }
                 double e2 = 0.0, tn[SPL][2];
+                int vmode = -1;  // mode whose Voce increment is in voce (systems of one mode share it)
+                double voce = 0.0;
 #pragma unroll
                 for (int k = 0; k < SPL; k++) {
                     const int s = r + 6 * k;
@@ -1441,11 +1443,13 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                             mode++;
                             last += ph.nsm[mode];
                         }
-                        const double tau1 = ph.tau1[mode], thet0 = ph.thet0[mode], thet1 = ph.thet1[mode];
-                        const double fact = fabs(thet0 / tau1);
-                        const double exp0 = exp(-fact * gamma0), exp1 = exp(-fact * gamma1);
-                        const double voce =
-                            deltgam * thet1 + tau1 * (exp0 - exp1) + thet1 * (gamma0 * exp0 - gamma1 * exp1);
+                        if (mode != vmode) {
+                            const double tau1 = ph.tau1[mode], thet0 = ph.thet0[mode], thet1 = ph.thet1[mode];
+                            const double fact = fabs(thet0 / tau1);
+                            const double exp0 = exp(-fact * gamma0), exp1 = exp(-fact * gamma1);
+                            voce = deltgam * thet1 + tau1 * (exp0 - exp1) + thet1 * (gamma0 * exp0 - gamma1 * exp1);
+                            vmode = mode;
+                        }
                         double dtau = 0.0;
 #pragma unroll
                         for (int js = 0; js < 6 * SPL; js++)

@@ -145,6 +145,11 @@ public:
     long long h2d = 0, d2h = 0;
     bool profile = false, write_vtk_files = false;
     int prec = 0;  // 1: mixed precision (FP32 spectrum, FFTs and Green operator in the equilibrium chain)
+    // Mixed precision falls back to FP64 for the rest of an increment once its FP32 iterations stop
+    // reducing the error: the FP32 round-off of the Green-operator update is about 1e-7 of the stress
+    // heterogeneity, which can exceed the tolerance when the strain rates are very small (slow creep).
+    int prec_it = 0;
+    std::vector<double> err_hist;
     struct KTime {
         std::string name;
         long long n = 0;
@@ -522,14 +527,14 @@ public:
     void equilibrium_iteration(bool fresh_sgavg) {
         ProcessData& p = P();
         if (fresh_sgavg) K("k_sgavg", [&] { launch_sgavg(d, st); });
-        K("k_fft_x_fwd", [&] { launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st, prec); });
-        K("k_fft_y_fwd", [&] { launch_fft_y(d, pl2, 9, false, st, prec); });
-        K("k_fft_z_green", [&] { launch_fft_z_green(d, pl3, d_c0, d_s0, st, prec); });
-        K("k_fft_y_inv", [&] { launch_fft_y(d, pl2, 9, true, st, prec); });
+        K("k_fft_x_fwd", [&] { launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st, prec_it); });
+        K("k_fft_y_fwd", [&] { launch_fft_y(d, pl2, 9, false, st, prec_it); });
+        K("k_fft_z_green", [&] { launch_fft_z_green(d, pl3, d_c0, d_s0, st, prec_it); });
+        K("k_fft_y_inv", [&] { launch_fft_y(d, pl2, 9, true, st, prec_it); });
         XinvParams xp;
         std::memcpy(xp.dvelgradavg, dvelgradavg, sizeof(xp.dvelgradavg));
         if (inv3(dinvc, xp.dinv) != 0) throw SolveError("Singular matrix in lu_inverse (correction_to_current)", -3);
-        K("k_fft_x_inv", [&] { launch_fft_x_inv(d, pl1, 0, xp, st, prec); });
+        K("k_fft_x_inv", [&] { launch_fft_x_inv(d, pl1, 0, xp, st, prec_it); });
         CorrParams cp;
         cp.mix = mix;
         cp.Lscale = std::max(lvmavg, EVP_TINY);
@@ -623,6 +628,8 @@ public:
                 mix = 1.0;
                 erre = 2.0 * p.error; errs = 2.0 * p.error; errsbc = 2.0 * p.error;
                 fresh = true;
+                prec_it = prec;
+                err_hist.clear();
             }
             iter++;
             total_iters++;
@@ -639,6 +646,11 @@ public:
                 p.tdotref = p.tdot;
             }
             if (errs <= p.error && erre <= p.error && errsbc <= p.error) did_converge = true;
+            if (prec_it != 0 && !did_converge) {  // FP32 stagnating above the tolerance: FP64 from here on
+                err_hist.push_back(std::max(errs, std::max(erre, errsbc)));
+                const size_t h = err_hist.size();
+                if (h >= 4 && err_hist[h - 1] > 0.7 * err_hist[h - 4]) prec_it = 0;
+            }
             if (p.ictrl == -1) {
                 if (p.tdot > p.tdotmin) {
                     double md;
