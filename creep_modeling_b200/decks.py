@@ -40,6 +40,15 @@ FCC_SLIP = [
 ]
 
 
+# BCC {110}<111> and {112}<111>: 24 systems in two modes (plane normal, slip direction)
+BCC_110 = [(0, 1, 1, 1, 1, -1), (0, 1, 1, 1, -1, 1), (0, 1, -1, 1, 1, 1), (0, 1, -1, -1, 1, 1),
+           (1, 0, 1, 1, 1, -1), (1, 0, 1, -1, 1, 1), (1, 0, -1, 1, 1, 1), (1, 0, -1, 1, -1, 1),
+           (1, 1, 0, 1, -1, 1), (1, 1, 0, -1, 1, 1), (1, -1, 0, 1, 1, 1), (1, -1, 0, 1, 1, -1)]
+BCC_112 = [(1, 1, 2, 1, 1, -1), (-1, 1, 2, 1, -1, 1), (1, -1, 2, -1, 1, 1), (1, 1, -2, 1, 1, 1),
+           (1, 2, 1, 1, -1, 1), (-1, 2, 1, 1, 1, -1), (1, 2, -1, -1, 1, 1), (1, -2, 1, 1, 1, 1),
+           (2, 1, 1, -1, 1, 1), (-2, 1, 1, 1, 1, 1), (2, 1, -1, 1, -1, 1), (2, -1, 1, 1, 1, -1)]
+
+
 @dataclasses.dataclass
 class Material:
     c11: float = 250000.0
@@ -54,6 +63,7 @@ class Material:
     thet1: float = 20.0
     hself: float = 1.0
     hlat: float = 1.4
+    slip: str = "fcc"  # "fcc": {111}<110>, 12 systems; "bcc24": {110}<111> + {112}<111>, 24 systems in two modes
 
 
 @dataclasses.dataclass
@@ -171,6 +181,9 @@ def write_cuel(path: Path, m: Material | None = None, iso: int = 0, young: float
 
 
 def write_cupl2(path: Path, m: Material) -> None:
+    if m.slip == "bcc24":
+        _write_cupl2_bcc(path, m)
+        return
     rows = "\n".join(f"{a}    {b}   {c}      {d}    {e}    {f}" for a, b, c, d, e, f in FCC_SLIP)
     txt = ("SLIP SYSTEMS FOR CUBIC CRYSTAL\n"
            "CUBIC          icryst\n"
@@ -183,6 +196,23 @@ def write_cupl2(path: Path, m: Material) -> None:
            f"{m.tau0f!r}  {m.tau0b!r}   {m.tau1!r}   {m.thet0!r}  {m.thet1!r}  0  tau0xf,tau0xb,tau1x,thet0,thet1,hpfac\n"
            f"{m.hself!r}   {m.hlat!r}                                               hselfx,hlatex\n"
            f"{rows}\n")
+    Path(path).write_text(txt)
+
+
+def _write_cupl2_bcc(path: Path, m: Material) -> None:
+    """Two modes with the same power law and Voce parameters; latent hardening hlat between and within modes."""
+    txt = ("SLIP SYSTEMS FOR CUBIC CRYSTAL (BCC)\n"
+           "CUBIC          icryst\n"
+           "1.   1.   1.   crystal axes (cdim(i))\n"
+           "2              nmodesx (total # of modes listed in the file)\n"
+           "2              nmodes  (# of modes to be used in the calculation)\n"
+           "1  2           mode(i) (label of the modes to be used)\n")
+    for mode, (name, rows) in enumerate((("{110}<111>", BCC_110), ("{112}<111>", BCC_112)), start=1):
+        txt += (f"{name}   SLIP\n"
+                f"{mode}   12   {m.nrs:.8f}   {m.gamd0:.8e}   0.0  0                 modex,nsmx,nrsx,gamd0x,twshx,isectwx\n"
+                f"{m.tau0f!r}  {m.tau0b!r}   {m.tau1!r}   {m.thet0!r}  {m.thet1!r}  0  tau0xf,tau0xb,tau1x,thet0,thet1,hpfac\n"
+                f"{m.hself!r}   {m.hlat!r}   {m.hlat!r}                                 hselfx,hlatex(1:2)\n")
+        txt += "\n".join(f"{a}    {b}   {c}      {d}    {e}    {f}" for a, b, c, d, e, f in rows) + "\n"
     Path(path).write_text(txt)
 
 

@@ -78,3 +78,18 @@ def test_long_z_pencils_parity(tmp_path):
     parity.assert_rows_match(rg, ro, dg, do)
     for f in ("sg", "velgrad", "gamdot", "xnode"):
         assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
+
+
+def test_bcc24_two_modes_parity(tmp_path):
+    """24 slip systems in two modes (BCC {110}<111> + {112}<111>): the local solve's
+    four-systems-per-lane kernels and the per-mode Voce increments."""
+    case = decks.case_c1(nsteps=3)
+    case.material.slip = "bcc24"
+    case.n = 12
+    case.ngrains = 12
+    fft = _case(tmp_path, case)
+    for modal in (0, 1):
+        g, o, rg, ro, dg, do = parity.run_both(fft, 3, mix=1, modal=modal)
+        parity.assert_rows_match(rg, ro, dg, do)
+        for f in ("sg", "velgrad", "gamdot", "trialtau"):
+            assert parity.field_rel_err(g, o, f) <= parity.RTOL, (modal, f)
