@@ -37,7 +37,7 @@ enum : int {
     OFF_DU2 = 160,    // 9   average-velgrad fix of update_tensor_config
     OFF_UPD3 = 176,   // 30+13 averages, hardening sums, last solid voxel
     OFF_DIAG = 224,   // 24+ diagnostics reductions
-    OFF_C0 = 272,     // 117 macro tangent sums
+    OFF_C0 = 272,     // 72 macro tangent sums (b-basis dsg/de, PK1 tangent)
     OFF_KIN = 392,    // 4   kinematic increment maxima
     OFF_DC = 400,     // 18  DC of the grid-update spectrum (complex x 9)
     OFF_G0 = 420,     // 81  real-space Green operator at the origin

@@ -30,6 +30,7 @@ namespace evp {
 
 constexpr int kBlock = 256;
 constexpr int kNewtonBlock = 128;
+constexpr int kC0Block = 64;
 
 // ---------------------------------------------------------------- reductions
 // NS sums then NM maxima per thread -> one partial per block (stored field-major,
@@ -229,14 +230,62 @@ __global__ void __launch_bounds__(kBlock) k_sgavg(Dev d) {
 }
 void launch_sgavg(const Dev& d, cudaStream_t st) { k_sgavg<<<d.grid, kBlock, 0, st>>>(d); }
 
+// ---------------------------------------------------------------- b-basis congruence
+// For a 3x3 matrix M, T(M)_ag = <B^a, B^g M^T> (Frobenius product; B^0..B^5 the orthonormal
+// b-basis of chg_basis).  A fourth-order tensor with minor symmetries, c = sum B^g c66_gd B^d,
+// pulled back as p_ijkl = sum_mn c_imkn M_jm M_ln has the b-basis components T c66 T^T, so the
+// 3x3x3x3 expansion and its contraction (81 x 9 products) reduce to two 6x6 products.
+__device__ __forceinline__ void basis_T(const double* M, double* T) {
+    double Bg[9], P[9], col[6];
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+#pragma unroll
+        for (int c = 0; c < 9; c++) Bg[c] = 0.0;
+        if (g == 0) { Bg[0] = -EVP_RSQ2; Bg[4] = EVP_RSQ2; }
+        else if (g == 1) { Bg[0] = -EVP_RSQ6; Bg[4] = -EVP_RSQ6; Bg[8] = EVP_RSQ23; }
+        else if (g == 2) { Bg[5] = EVP_RSQ2; Bg[7] = EVP_RSQ2; }
+        else if (g == 3) { Bg[2] = EVP_RSQ2; Bg[6] = EVP_RSQ2; }
+        else if (g == 4) { Bg[1] = EVP_RSQ2; Bg[3] = EVP_RSQ2; }
+        else { Bg[0] = EVP_RSQ3; Bg[4] = EVP_RSQ3; Bg[8] = EVP_RSQ3; }
+        mm3_bt(Bg, M, P);  // B^g M^T
+        t2_to_b6(P, col);
+#pragma unroll
+        for (int a = 0; a < 6; a++) T[6 * a + g] = col[a];
+    }
+}
+// out = s * T A T^T (6x6)
+__device__ __forceinline__ void congruence6(const double* T, const double* A, double s, double* out) {
+    double TA[36];
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            double x = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; k++) x += T[6 * i + k] * A[6 * k + j];
+            TA[6 * i + j] = x;
+        }
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            double x = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; k++) x += TA[6 * i + k] * T[6 * j + k];
+            out[6 * i + j] = s * x;
+        }
+}
+
 // ---------------------------------------------------------------- k_prologue
 __global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __restrict__ c0g, const double* __restrict__ g0g,
                                                        int do_schmid, int modal) {
-    __shared__ double c0[81], g0[81];
+    __shared__ double c0[81], g0[81], c0b[36];
     for (int i = threadIdx.x; i < 81; i += blockDim.x) {
         c0[i] = c0g[i];
         g0[i] = modal ? g0g[i] : 0.0;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) t4_to_b66(c0, c0b);
     __syncthreads();
     const long long N = d.N;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
@@ -261,24 +310,11 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __rest
         }
         double F[9], detF = d.detF[v];
         ld9(d.F, N, v, F);
-        double cm[81], cs[81], c66[36];
-        for (int ii = 0; ii < 3; ii++)
-            for (int jj = 0; jj < 3; jj++)
-                for (int kk = 0; kk < 3; kk++)
-                    for (int ll = 0; ll < 3; ll++) {
-                        double dum = 0.0;
-                        for (int m = 0; m < 3; m++)
-                            for (int n = 0; n < 3; n++) dum += c0[((ii * 3 + m) * 3 + kk) * 3 + n] * F[3 * jj + m] * F[3 * ll + n];
-                        cm[((ii * 3 + jj) * 3 + kk) * 3 + ll] = dum / detF;
-                    }
-        for (int ii = 0; ii < 3; ii++)
-            for (int jj = 0; jj < 3; jj++)
-                for (int kk = 0; kk < 3; kk++)
-                    for (int ll = 0; ll < 3; ll++)
-                        cs[((ii * 3 + jj) * 3 + kk) * 3 + ll] =
-                            0.25 * (cm[((ii * 3 + jj) * 3 + kk) * 3 + ll] + cm[((jj * 3 + ii) * 3 + kk) * 3 + ll] +
-                                    cm[((ii * 3 + jj) * 3 + ll) * 3 + kk] + cm[((jj * 3 + ii) * 3 + ll) * 3 + kk]);
-        t4_to_b66(cs, c66);
+        // calc_c066mod: cm_ijkl = sum_mn c0_imkn F_jm F_ln / J, quarter-symmetrized, in the b-basis;
+        // c0 has the minor symmetries, so this is (1/J) T(F) c0_66 T(F)^T
+        double c66[36], TF[36];
+        basis_T(F, TF);
+        congruence6(TF, c0b, 1.0 / detF, c66);
         for (int c = 0; c < 36; c++) d.c066mod[c * N + v] = c66[c];
         {  // its inverse, for the symmetric form of the local Newton system
             double ci[36];
@@ -289,7 +325,7 @@ __global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __rest
             for (int c = 0; c < 36; c++) d.c066inv[c * N + v] = ci[c];
         }
         if (modal) {
-            double Fi[9], g66[36];
+            double Fi[9], g66[36], cm[81], cs[81];
             ld9(d.Finv, N, v, Fi);
             for (int ii = 0; ii < 3; ii++)
                 for (int jj = 0; jj < 3; jj++)
@@ -1996,11 +2032,12 @@ void launch_diag(const Dev& d, double Lfloor, cudaStream_t st) { k_diag<<<d.grid
 
 // ---------------------------------------------------------------- k_c0
 template <int NS>
-__global__ void __launch_bounds__(kBlock) k_c0(Dev d, double tdot, double tdotref) {
+__global__ void __launch_bounds__(kC0Block) k_c0(Dev d, double tdot, double tdotref) {
     const long long N = d.N;
-    double s[117];
-#pragma unroll
-    for (int c = 0; c < 117; c++) s[c] = 0.0;
+    // each thread's 72 running sums in its own shared-memory slice (registers hold the per-voxel work)
+    extern __shared__ double c0acc[];
+    double* const s = c0acc + threadIdx.x * 72;
+    for (int c = 0; c < 72; c++) s[c] = 0.0;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
         if (d.gas[v]) continue;
         const PhaseDev& ph = d.ph[d.phase[v]];
@@ -2015,31 +2052,36 @@ __global__ void __launch_bounds__(kBlock) k_c0(Dev d, double tdot, double tdotre
         }
         constitutive<NS>(ph, d.sch, N, v, tt, sg, ep, dd, gd);
         double tr[36];
+#pragma unroll
         for (int i = 0; i < 6; i++)
+#pragma unroll
             for (int j = 0; j < 6; j++) tr[6 * i + j] = d.sg66[(6 * i + j) * N + v] / tdot * tdot / tdotref + dd_at(dd, i, j);
         if (inv_unrolled<6>(tr) != 0) set_err(d.err, 1);
-        double dsg[81], dpg[81], dp6[36], Fi[9];
-        b66_to_t4(tr, dsg);
+        // dsg = tr in the b-basis (summed here, expanded to 3x3x3x3 on the host); the PK1 tangent
+        // dpg_ijkl = J sum_mn dsg_imkn Fi_jm Fi_ln has the b-basis components J T(Fi) tr T(Fi)^T
+        double Fi[9], T[36], dp6[36];
         ld9(d.Finv, N, v, Fi);
         const double detF = d.detF[v], w = d.wgtc[v];
-        for (int i = 0; i < 3; i++)
-            for (int j = 0; j < 3; j++)
-                for (int k = 0; k < 3; k++)
-                    for (int l = 0; l < 3; l++) {
-                        double x = 0.0;
-                        for (int m = 0; m < 3; m++)
-                            for (int n = 0; n < 3; n++) x = x + dsg[((i * 3 + m) * 3 + k) * 3 + n] * Fi[3 * j + m] * Fi[3 * l + n] * detF;
-                        dpg[((i * 3 + j) * 3 + k) * 3 + l] = x;
-                    }
-        t4_to_b66(dpg, dp6);
-        for (int c = 0; c < 81; c++) s[c] += dsg[c] * w;
-        for (int c = 0; c < 36; c++) s[81 + c] += dp6[c] * d.wgt;
+        basis_T(Fi, T);
+        congruence6(T, tr, detF, dp6);
+#pragma unroll
+        for (int c = 0; c < 36; c++) s[c] += tr[c] * w;
+#pragma unroll
+        for (int c = 0; c < 36; c++) s[36 + c] += dp6[c] * d.wgt;
     }
-    reduce_store<117, 0>(s, nullptr, d.partials, d.red + OFF_C0, d.counters + CNT_C0);
+    reduce_store<72, 0>(s, nullptr, d.partials, d.red + OFF_C0, d.counters + CNT_C0);
 }
 void launch_c0(const Dev& d, double tdot, double tdotref, cudaStream_t st) {
-    if (d.nsys <= 12) k_c0<12><<<d.grid, kBlock, 0, st>>>(d, tdot, tdotref);
-    else k_c0<24><<<d.grid, kBlock, 0, st>>>(d, tdot, tdotref);
+    const size_t sm = (size_t)kC0Block * 72 * sizeof(double);
+    const long long g = (d.N + kC0Block - 1) / kC0Block;
+    const int grid = (int)(g < 148LL * 16 ? g : 148LL * 16);
+    if (d.nsys <= 12) {
+        cudaFuncSetAttribute(k_c0<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_c0<12><<<grid, kC0Block, sm, st>>>(d, tdot, tdotref);
+    } else {
+        cudaFuncSetAttribute(k_c0<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_c0<24><<<grid, kC0Block, sm, st>>>(d, tdot, tdotref);
+    }
 }
 
 // ---------------------------------------------------------------- k_kinematic

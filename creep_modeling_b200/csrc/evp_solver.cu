@@ -857,10 +857,9 @@ public:
 
     void finish_c0(const ProcessData& p) {  // calc_c0 tail (various_functions.f90:2633-2647)
         const double* r = h_red + OFF_C0;
-        double dsde[81], dP[36], a[36], ai[36];
-        for (int c = 0; c < 81; c++) dsde[c] = r[c] / wphcsol;
-        for (int c = 0; c < 36; c++) dP[c] = r[81 + c] / wphsol;
-        t4_to_b66(dsde, a);
+        double dP[36], a[36], ai[36];
+        for (int c = 0; c < 36; c++) a[c] = r[c] / wphcsol;  // <dsg/de> in the b-basis
+        for (int c = 0; c < 36; c++) dP[c] = r[36 + c] / wphsol;
         std::memcpy(ai, a, sizeof(a));
         if (lu_inverse(ai, 6) != 0) throw SolveError("Singular matrix in lu_inverse (calc_c0)", -3);
         b66_to_t4(ai, de_ds);
