@@ -230,7 +230,7 @@ def serving_sample(k: int, scale: float, rate: float) -> dict:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=64, help="grid edge (default: the 64^3 configuration)")
@@ -334,25 +334,32 @@ def main(argv=None) -> int:
                 "kernel_share": {k: round(v[1] / max(sum(x[1] for x in kd.values()), 1e-30), 4) for k, v in
                                  sorted(kd.items(), key=lambda kv: -kv[1][1])}}
 
-    # end to end through the C ABI with host buffers: deck files -> device -> CSV rows
+    # end to end through the C ABI with host buffers: deck files -> device -> CSV rows (median of 3 runs)
     e2e = None
     try:
-        with tempfile.TemporaryDirectory() as td2:
-            fft2 = make_deck(Path(td2), n, args.steps + 1, args.ngrains)
-            out = Path(td2) / "out"
-            torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
-            s2 = Solve(fft2, out_dir=out, mix=1, modal=0, csv_only=True)
-            for _ in range(args.steps):
-                s2.advance(1)
-            r2 = s2.stats()
-            s2.close()
-            torch.cuda.synchronize(dev)
-            we = time.perf_counter() - t0
-            e2e = {"value": r2.voxel_iters / we, "unit": METRIC,
-                   "h2d_bytes_per_step": int(r2.h2d_bytes / max(args.steps, 1)),
-                   "d2h_bytes_per_step": int(r2.d2h_bytes / max(args.steps, 1)),
-                   "note": "evp_open (deck files parsed and uploaded) + steps + results/diagnostics CSV rows, host wall clock"}
+        runs = []
+        for rep in range(3):
+            with tempfile.TemporaryDirectory() as td2:
+                fft2 = make_deck(Path(td2), n, args.steps + 1, args.ngrains)
+                out = Path(td2) / "out"
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                s2 = Solve(fft2, out_dir=out, mix=1, modal=0, csv_only=True)
+                for _ in range(args.steps):
+                    s2.advance(1)
+                r2 = s2.stats()
+                s2.close()
+                torch.cuda.synchronize(dev)
+                we = time.perf_counter() - t0
+                runs.append((r2.voxel_iters / we, r2))
+        runs.sort(key=lambda x: x[0])
+        val, r2 = runs[1]
+        e2e = {"value": val, "unit": METRIC,
+               "h2d_bytes_per_step": int(r2.h2d_bytes / max(args.steps, 1)),
+               "d2h_bytes_per_step": int(r2.d2h_bytes / max(args.steps, 1)),
+               "runs": [round(x[0], 1) for x in runs],
+               "note": "evp_open (deck files parsed and uploaded) + steps + results/diagnostics CSV rows, host wall "
+                       "clock; median of 3 runs"}
     except Exception as exc:  # pragma: no cover - reported, not hidden
         e2e = {"value": None, "unit": METRIC, "error": str(exc)}
 
