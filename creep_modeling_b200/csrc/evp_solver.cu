@@ -120,6 +120,7 @@ public:
     double last_results[53] = {}, last_diag[44] = {};
     std::vector<double> snap_dsim, snap_scau;
     bool has_thermo = false;
+    std::vector<double> eth_soa;  // host staging of the thermal eigenstrain upload (kept until the copy completes)
 
     ProcessData& P() { return dk.process[ipr - 1]; }
 
@@ -378,7 +379,12 @@ public:
         }
         h2d_copy(d.gas, gas.data(), N);
         h2d_copy(d.phase, phs.data(), N);
-        if (d.eth) h2d_copy(d.eth, dk.eth.data(), 9 * N * sizeof(double));
+        if (d.eth) {  // the deck keeps eth voxel-major (9 per voxel); the device field is component-major
+            eth_soa.resize(9 * (size_t)N);
+            for (long long v = 0; v < N; v++)
+                for (int c = 0; c < 9; c++) eth_soa[(size_t)c * N + v] = dk.eth[9 * (size_t)v + c];
+            h2d_copy(d.eth, eth_soa.data(), 9 * N * sizeof(double));
+        }
         for (auto& p : dk.process) has_thermo = has_thermo || p.ithermo == 1;
         double* d_eul = dalloc<double>(3 * N);
         int* d_gr = dalloc<int>(N);

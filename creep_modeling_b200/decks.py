@@ -86,6 +86,7 @@ class Loading:
     xc0: float = 2.0
     igamma: int = 0
     ictrl: int = -1
+    thermo_file: str | None = None  # ITHERMO = 1 with this per-grain eigenstrain file
 
 
 def _nearest_seed(pts: np.ndarray, seeds: np.ndarray, box: np.ndarray) -> np.ndarray:
@@ -265,7 +266,8 @@ def _process_block(p: Loading) -> str:
             "1               IWTEX (write texture at the end)\n"
             f"{p.iwfields} {p.iwstep}            IWFIELDS,IWSTEP (write fields, and frequency of writing)\n"
             f"{p.xc0!r} {p.igamma}            XC0, IGAMMA (0-continious,1-discrete central diff,2-rotated)\n"
-            "0               ITHERMO (if ithermo=1, next line is filethermo)\n")
+            + ("0               ITHERMO (if ithermo=1, next line is filethermo)\n" if p.thermo_file is None else
+               f"1               ITHERMO (if ithermo=1, next line is filethermo)\n{p.thermo_file}\n"))
 
 
 def write_fft_in(path: Path, n, micro: Path, cupl2: Path, cuel: Path, processes: list[Loading],
@@ -307,6 +309,9 @@ class Case:
     material: Material
     processes: list
     phase2_frac: float = 0.0
+    phase2_gas: bool = False  # the second phase as gas (igas = 1) instead of the stiff elastic phase
+    complgas: float = 0.0
+    thermo_eigenstrain: float = 0.0  # > 0: per-grain thermal eigenstrain of this size (ITHERMO = 1)
 
 
 def case_c1(nsteps: int = 100) -> Case:
@@ -342,10 +347,24 @@ def write_case(case: Case, root: Path, micro_cache: dict | None = None) -> Path:
         write_cuel(root / "cuel2.sx", iso=1, young=400000.0, nu=0.3)
         m2 = dataclasses.replace(case.material, tau0f=1e8, tau0b=1e8)
         write_cupl2(root / "cupl2_2.sx", m2)
-        phase2 = (0, root / "cupl2_2.sx", root / "cuel2.sx")
+        phase2 = (1 if case.phase2_gas else 0, root / "cupl2_2.sx", root / "cuel2.sx")
+    processes = case.processes
+    if case.thermo_eigenstrain > 0.0:
+        write_thermo(root / "thermo.txt", case.ngrains, case.thermo_eigenstrain, case.seed)
+        processes = [dataclasses.replace(p, thermo_file=str(root / "thermo.txt")) for p in processes]
     fft = root / "fft.in"
-    write_fft_in(fft, case.n, micro, root / "cupl2.sx", root / "cuel.sx", case.processes, phase2=phase2)
+    write_fft_in(fft, case.n, micro, root / "cupl2.sx", root / "cuel.sx", processes, phase2=phase2,
+                 complgas=case.complgas)
     return fft
+
+
+def write_thermo(path: Path, ngrains: int, size: float, seed: int) -> None:
+    """Per-grain thermal eigenstrain file read after ITHERMO = 1: the grain count, then one line
+    of e11 e22 e33 e23 e13 e12 per grain (seeded, components uniform in [-size, size])."""
+    rng = np.random.default_rng([seed, 7])
+    e = rng.uniform(-size, size, size=(ngrains, 6))
+    lines = [str(ngrains)] + [" ".join(f"{x:.10e}" for x in row) for row in e]
+    Path(path).write_text("\n".join(lines) + "\n")
 
 
 def case_c4(i: int, nsteps: int = 150) -> Case:

@@ -93,3 +93,47 @@ def test_bcc24_two_modes_parity(tmp_path):
         parity.assert_rows_match(rg, ro, dg, do)
         for f in ("sg", "velgrad", "gamdot", "trialtau"):
             assert parity.field_rel_err(g, o, f) <= parity.RTOL, (modal, f)
+
+
+def test_gas_phase_parity(tmp_path):
+    """A second phase of gas voxels (igas = 1; closed-form stress update with the gas compliance)."""
+    case = decks.case_c1(nsteps=3)
+    case.n = 16
+    case.ngrains = 20
+    case.phase2_frac = 0.05
+    case.phase2_gas = True
+    case.complgas = 1.0
+    fft = _case(tmp_path, case)
+    g, o, rg, ro, dg, do = parity.run_both(fft, 3)
+    parity.assert_rows_match(rg, ro, dg, do)
+    for f in ("sg", "velgrad", "gamdot"):
+        assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
+
+
+def test_thermal_eigenstrain_parity(tmp_path):
+    """ITHERMO = 1: a per-grain thermal eigenstrain rate in the first increment's local solve."""
+    case = decks.case_c1(nsteps=3)
+    case.n = 12
+    case.ngrains = 16
+    case.thermo_eigenstrain = 1e-5
+    fft = _case(tmp_path, case)
+    g, o, rg, ro, dg, do = parity.run_both(fft, 3)
+    parity.assert_rows_match(rg, ro, dg, do)
+    for f in ("sg", "velgrad", "gamdot"):
+        assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
+
+
+def test_substep_rollback_parity(tmp_path):
+    """Time control (ICTRL = -1) with tdotmin < tdot and a small itmax: increments that do not
+    converge in itmax iterations roll back and are cut into kinematic substeps."""
+    case = decks.case_c1(nsteps=4)
+    case.n = 12
+    case.ngrains = 16
+    case.processes[0].itmax = 4
+    case.processes[0].tdotmin = 2.5
+    fft = _case(tmp_path, case)
+    g, o, rg, ro, dg, do = parity.run_both(fft, 12)
+    parity.assert_rows_match(rg, ro, dg, do)
+    assert len(rg) > 4  # substeps were taken
+    for f in ("sg", "velgrad", "gamdot"):
+        assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
