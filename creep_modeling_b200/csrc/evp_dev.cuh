@@ -77,10 +77,14 @@ struct Dev {
     double2 *tw1, *tw2, *tw3;
     float2 *tw1f, *tw2f, *tw3f;  // FP32 twiddles of the mixed-precision path (may be null)
     double *dv3, *xnode;
+    // tabulated Green operator of IGAMMA 1 and 2: 81 components per half-spectrum point,
+    // goper[c * (n1h n2 n3) + (k3 n2 + j) n1h + kx]; gtab = 1 while the current process uses it
+    double* goper;
+    int gtab;
     // reductions
     double *partials, *red;
     unsigned int *counters;
-    int *err;  // error word: bit 0 singular matrix, bit 1 non-finite Newton result
+    int *err;  // error word: bit 0 singular matrix, bit 1 non-finite Newton result, bit 2 form_G failure
     const PhaseDev *ph;
     int nph;
 };
@@ -115,7 +119,9 @@ void launch_init(const Dev& d, const double* euler, const int* grain, const doub
                  cudaStream_t st);
 void launch_sgavg(const Dev& d, cudaStream_t st);
 void launch_prologue(const Dev& d, const double* c0, const double* goperr0, int do_schmid, int modal, cudaStream_t st);
-void launch_goperr0(const Dev& d, const double* c0, const double* s0, cudaStream_t st);
+void launch_goperr0(const Dev& d, const double* c0, const double* s0, int igamma, cudaStream_t st);
+// form_G for IGAMMA 1 and 2: tabulate the Green operator at every half-spectrum point
+void launch_goper_tab(const Dev& d, const double* c0, const double* s0, int igamma, cudaStream_t st);
 void launch_gas_compl(const Dev& d, double tdot, double complgas, int modal, cudaStream_t st);
 void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st);
 void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st);

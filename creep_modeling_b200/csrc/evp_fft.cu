@@ -352,7 +352,20 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_green(Dev d, Fft
 #pragma unroll
         for (int c = 0; c < 9; c++) a[c] = q[c * T];
         const bool nyq = (n1 % 2 == 0 && kx == n1 / 2) || nyq_y || (n3 % 2 == 0 && k3 == n3 / 2 && n3 > 1);
-        if (kx == 0 && j == 0 && k3 == 0) {
+        if (d.gtab) {  // IGAMMA 1 or 2: the tabulated operator, r_pq = Gamma_pqij a_ij
+            const long long P = (long long)n1h * n2 * n3, pt = ((long long)k3 * n2 + j) * n1h + kx;
+#pragma unroll
+            for (int pq = 0; pq < 9; pq++) {
+                CT acc = mk<CT>(0, 0);
+#pragma unroll
+                for (int ij = 0; ij < 9; ij++) {
+                    const Re g = (Re)d.goper[(pq * 9 + ij) * P + pt];
+                    acc.x += g * a[ij].x;
+                    acc.y += g * a[ij].y;
+                }
+                r[pq] = acc;
+            }
+        } else if (kx == 0 && j == 0 && k3 == 0) {
 #pragma unroll
             for (int c = 0; c < 9; c++) r[c] = mk<CT>(0, 0);
         } else if (nyq) {

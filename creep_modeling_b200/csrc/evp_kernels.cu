@@ -2146,7 +2146,6 @@ void launch_cell2node(const Dev& d, double tdot, int ideriv, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------- k_goperr0
-// Goperr0 = (1/N) sum_k Re Gamma(k) over the full grid (igamma = 0).
 __device__ __forceinline__ void spatial_freq(int kx, int ky, int kz, int n1, int n2, int n3, double* xi) {
     const double twopi = 2.0 * EVP_PI;
     xi[0] = (kx + 1 <= n1 / 2) ? twopi * (double)kx / (double)n1 : twopi * (double)(kx - n1) / (double)n1;
@@ -2154,7 +2153,109 @@ __device__ __forceinline__ void spatial_freq(int kx, int ky, int kz, int n1, int
     if (n3 == 1) xi[2] = 0.0;
     else xi[2] = (kz + 1 <= n3 / 2) ? twopi * (double)kz / (double)n3 : twopi * (double)(kz - n3) / (double)n3;
 }
-__global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restrict__ c0g, const double* __restrict__ s0g) {
+// Green operator at one frequency point, all three forms of form_G (various_functions.f90:640-785):
+// IGAMMA 0 continuous (Nyquist planes: -s0), 1 discrete central differences followed by four
+// projections g <- -g1 : c0 : g, 2 rotated scheme (zero where two Nyquist planes meet).
+// kx, ky, kz are 0-based indices of the full spectrum.  Returns 1 for a singular acoustic tensor
+// or a complex rotated-scheme D (the reference stops there).
+__device__ int goper_at(int igamma, int kx, int ky, int kz, int n1, int n2, int n3, const double* c0, const double* s0,
+                        double* g) {
+    const bool nx = (n1 % 2 == 0 && kx == n1 / 2), ny = (n2 % 2 == 0 && ky == n2 / 2), nz = (n3 % 2 == 0 && kz == n3 / 2);
+    if ((nx || ny || (nz && n3 > 1)) && igamma == 0) {
+        for (int c = 0; c < 81; c++) g[c] = -s0[c];
+        return 0;
+    }
+    if (((nx && ny) || (nx && nz) || (ny && nz)) && igamma >= 2) {
+        for (int c = 0; c < 81; c++) g[c] = 0.0;
+        return 0;
+    }
+    int bad = 0;
+    double xk[3], D[9];
+    spatial_freq(kx, ky, kz, n1, n2, n3, xk);
+    if (igamma == 0) {
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) D[3 * i + j] = xk[i] * xk[j];
+    } else if (igamma == 1) {
+        const double twopi = 2.0 * EVP_PI;
+        const double xi = twopi * (double)kx / (double)n1, xj = twopi * (double)ky / (double)n2,
+                     xz = twopi * (double)kz / (double)n3;
+        D[0] = 2.0 * (cos(xi) - 1.0);
+        D[4] = 2.0 * (cos(xj) - 1.0);
+        D[8] = 2.0 * (cos(xz) - 1.0);
+        D[3] = -sin(xi) * sin(xj);
+        D[6] = -sin(xi) * sin(xz);
+        D[7] = -sin(xj) * sin(xz);
+        D[1] = D[3];
+        D[2] = D[6];
+        D[5] = D[7];
+    } else {
+        // kmod = i/4 (1 + e^{i xk1})(1 + e^{i xk2})(1 + e^{i xk3}) tan(xk/2); D = Re(kmod kmod^*)
+        double br = 0.0, bi = 0.25;
+        for (int l = 0; l < 3; l++) {
+            const double fr = 1.0 + cos(xk[l]), fi = sin(xk[l]);
+            const double r = br * fr - bi * fi, im = br * fi + bi * fr;
+            br = r;
+            bi = im;
+        }
+        double kr[3], ki[3];
+        for (int l = 0; l < 3; l++) {
+            const double t = tan(xk[l] / 2.0);
+            kr[l] = t * br;
+            ki[l] = t * bi;
+        }
+        double im2 = 0.0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                D[3 * i + j] = kr[i] * kr[j] + ki[i] * ki[j];
+                const double dim = ki[i] * kr[j] - kr[i] * ki[j];
+                im2 += dim * dim;
+            }
+        if (sqrt(im2) > 1.0e-7) bad = 1;
+    }
+    double a[9];
+    if (kx == 0 && ky == 0 && kz == 0) {
+        for (int c = 0; c < 9; c++) a[c] = 0.0;
+    } else {
+        double A[9];
+        for (int i = 0; i < 3; i++)
+            for (int k = 0; k < 3; k++) {
+                double x = 0.0;
+                for (int j = 0; j < 3; j++)
+                    for (int l = 0; l < 3; l++) x += c0[((i * 3 + j) * 3 + k) * 3 + l] * D[3 * j + l];
+                A[3 * i + k] = x;
+            }
+        if (inv3u(A, a) != 0) bad = 1;
+    }
+    for (int p = 0; p < 3; p++)
+        for (int q = 0; q < 3; q++)
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) g[((p * 3 + q) * 3 + i) * 3 + j] = -a[3 * p + i] * D[3 * q + j];
+    if (igamma == 1) {
+        // g <- -g1 : (c0 : g) four times, as two 9x9 products (the four-fold sum regrouped)
+        double g1[81], t[81];
+        for (int c = 0; c < 81; c++) g1[c] = g[c];
+        for (int itt = 0; itt < 4; itt++) {
+            for (int mn = 0; mn < 9; mn++)
+                for (int kl = 0; kl < 9; kl++) {
+                    double x = 0.0;
+                    for (int op = 0; op < 9; op++) x += c0[mn * 9 + op] * g[op * 9 + kl];
+                    t[mn * 9 + kl] = x;
+                }
+            for (int ij = 0; ij < 9; ij++)
+                for (int kl = 0; kl < 9; kl++) {
+                    double x = 0.0;
+                    for (int mn = 0; mn < 9; mn++) x += g1[ij * 9 + mn] * t[mn * 9 + kl];
+                    g[ij * 9 + kl] = -x;
+                }
+        }
+    }
+    return bad;
+}
+
+// Real-space origin value of the Green operator (mean over the full spectrum), used by the
+// modified augmented Lagrangian (various_functions.f90:798-807).
+__global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restrict__ c0g, const double* __restrict__ s0g,
+                                                    int igamma) {
     __shared__ double c0[81], s0[81];
     for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = c0g[i]; s0[i] = s0g[i]; }
     __syncthreads();
@@ -2165,6 +2266,12 @@ __global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restr
     for (int c = 0; c < 81; c++) s[c] = 0.0;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
         const int kx = (int)(v % n1), ky = (int)((v / n1) % n2), kz = (int)(v / ((long long)n1 * n2));
+        if (igamma != 0) {
+            double g[81];
+            if (goper_at(igamma, kx, ky, kz, n1, n2, n3, c0, s0, g) != 0) set_err(d.err, 4);
+            for (int c = 0; c < 81; c++) s[c] += g[c];
+            continue;
+        }
         const bool nyq = (n1 % 2 == 0 && kx == n1 / 2) || (n2 % 2 == 0 && ky == n2 / 2) || (n3 % 2 == 0 && kz == n3 / 2 && n3 > 1);
         if (nyq) {
             for (int c = 0; c < 81; c++) s[c] += -s0[c];
@@ -2188,8 +2295,27 @@ __global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restr
     }
     reduce_store<81, 0>(s, nullptr, d.partials, d.red + OFF_G0, d.counters + CNT_G0);
 }
-void launch_goperr0(const Dev& d, const double* c0, const double* s0, cudaStream_t st) {
-    k_goperr0<<<d.grid, kBlock, 0, st>>>(d, c0, s0);
+void launch_goperr0(const Dev& d, const double* c0, const double* s0, int igamma, cudaStream_t st) {
+    k_goperr0<<<d.grid, kBlock, 0, st>>>(d, c0, s0, igamma);
+}
+
+// form_G for IGAMMA 1 and 2 on the half spectrum, once per increment (c0 changes per increment)
+__global__ void __launch_bounds__(kBlock) k_goper_tab(Dev d, const double* __restrict__ c0g, const double* __restrict__ s0g,
+                                                      int igamma) {
+    __shared__ double c0[81], s0[81];
+    for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = c0g[i]; s0[i] = s0g[i]; }
+    __syncthreads();
+    const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
+    const long long P = (long long)n1h * n2 * n3;
+    for (long long pt = blockIdx.x * (long long)blockDim.x + threadIdx.x; pt < P; pt += (long long)gridDim.x * blockDim.x) {
+        const int kx = (int)(pt % n1h), j = (int)((pt / n1h) % n2), k3 = (int)(pt / ((long long)n1h * n2));
+        double g[81];
+        if (goper_at(igamma, kx, j, k3, d.n1, n2, n3, c0, s0, g) != 0) set_err(d.err, 4);
+        for (int c = 0; c < 81; c++) d.goper[c * P + pt] = g[c];
+    }
+}
+void launch_goper_tab(const Dev& d, const double* c0, const double* s0, int igamma, cudaStream_t st) {
+    k_goper_tab<<<d.grid, kBlock, 0, st>>>(d, c0, s0, igamma);
 }
 
 }  // namespace evp

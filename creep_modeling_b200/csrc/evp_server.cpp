@@ -54,14 +54,16 @@ bool deck_grid(const std::string& fft, int& n1, int& n2, int& n3) {
 // Device memory of one solve, from the solver's allocations with the largest
 // slip-system count (24) and every optional field present: about 5.3 kB per
 // voxel of state, the half spectrum (9 complex values per half-spectrum point),
-// the node coordinates and fixed buffers.
+// the tabulated Green operator of IGAMMA 1 and 2 (81 doubles per half-spectrum
+// point), the node coordinates and fixed buffers.
 unsigned long long footprint(int n1, int n2, int n3) {
     const unsigned long long N = (unsigned long long)n1 * n2 * n3;
     const unsigned long long per_voxel = 660ull * 8ull;
     const unsigned long long spec = 9ull * 16ull * (unsigned long long)(n1 / 2 + 1) * n2 * n3;
+    const unsigned long long goper = 81ull * 8ull * (unsigned long long)(n1 / 2 + 1) * n2 * n3;
     const unsigned long long nodes = 3ull * 8ull * (n1 + 1ull) * (n2 + 1ull) * (n3 + 1ull);
     const unsigned long long partials = 8ull * (200ull * 2048ull + 9ull * ((unsigned long long)n2 * n3 / 2 + 1));
-    return N * per_voxel + spec + nodes + partials + (1ull << 20);
+    return N * per_voxel + spec + goper + nodes + partials + (1ull << 20);
 }
 
 double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); }

@@ -205,6 +205,7 @@ public:
         resolve_timers();
         if (*h_err & 1) throw SolveError("singular matrix in a voxel operator (lu_inverse / lu_eqsystem)", -3);
         if (*h_err & 2) throw SolveError("non-finite stress in the local Newton solve", -4);
+        if (*h_err & 4) throw SolveError("form_G failed (singular acoustic tensor or complex D operator)", -3);
     }
 
     // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
@@ -226,8 +227,6 @@ public:
         } catch (DeckError& e) {
             throw SolveError(e.what(), e.code);
         }
-        for (auto& p : dk.process)
-            if (p.igamma != 0) throw SolveError("IGAMMA = 1 or 2 (discrete Green operators) is not supported by this build", -2);
         int dev_count = 0;
         if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) throw SolveError("no CUDA device available", -6);
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -288,6 +287,12 @@ public:
         d.s_velgrad = dalloc<double>(9 * N); d.s_velgradold = dalloc<double>(9 * N); d.s_sg = dalloc<double>(6 * N);
         d.s_edotp = dalloc<double>(6 * N); d.s_gamdot = dalloc<double>((size_t)ns * N); d.s_trialtau = dalloc<double>(2 * (size_t)ns * N);
         d.spec = dalloc<double2>(9 * (size_t)d.n1h * dk.n2 * dk.n3);
+        {
+            bool any_tab = false;
+            for (auto& p : dk.process) any_tab = any_tab || p.igamma != 0;
+            d.goper = any_tab ? dalloc<double>(81 * (size_t)d.n1h * dk.n2 * dk.n3) : nullptr;
+            d.gtab = 0;
+        }
         d.tw1 = dalloc<double2>(dk.n1); d.tw2 = dalloc<double2>(dk.n2); d.tw3 = dalloc<double2>(dk.n3);
         d.dv3 = dalloc<double>(3 * N);
         d.xnode = dalloc<double>(3 * (size_t)(dk.n1 + 1) * (dk.n2 + 1) * d.n3node);
@@ -617,8 +622,10 @@ public:
         snapshot(true);
         bool did_converge = false, accept_step = false;
         const int do_schmid = ((imicro == 1 && ipr == 1) || p.iupdate == 1) ? 1 : 0;
-        if (modal) {  // form_G: only the real-space origin value is needed (Gamma is applied on the fly)
-            K("k_goperr0", [&] { launch_goperr0(d, d_c0, d_s0, st); });
+        d.gtab = (p.igamma != 0 && d.goper) ? 1 : 0;
+        if (d.gtab) K("k_goper_tab", [&] { launch_goper_tab(d, d_c0, d_s0, p.igamma, st); });  // form_G, IGAMMA 1, 2
+        if (modal) {  // form_G: the real-space origin value (IGAMMA 0 is applied on the fly)
+            K("k_goperr0", [&] { launch_goperr0(d, d_c0, d_s0, p.igamma, st); });
             fetch_red();
             for (int c = 0; c < 81; c++) goperr0[c] = h_red[OFF_G0 + c] / (double)d.N;
             h2d_copy(d_g0, goperr0, sizeof(goperr0));

@@ -52,7 +52,7 @@ def test_valid_deck_reaches_device_check(tmp_path):
 @pytest.mark.parametrize("mutate,code,needle", [
     (lambda s: s.replace("\t1       1       0                     |            \n",
                          "\t1       1       1                     |            \n", 1), -1, "boundary"),
-    (lambda s: s.replace("2.0 0            XC0", "2.0 1            XC0", 1), -2, "IGAMMA"),
+    (lambda s: s.replace("2.0 0            XC0", "2.0 3            XC0", 1), -1, "igamma"),
     (lambda s: s.replace("0                      IDISPINI", "1                      IDISPINI", 1), -2, "IDISPINI"),
 ])
 def test_invalid_decks_are_refused(tmp_path, mutate, code, needle):
@@ -61,6 +61,16 @@ def test_invalid_decks_are_refused(tmp_path, mutate, code, needle):
     rc, msg = _open(fft)
     assert rc == code, msg
     assert needle.lower() in msg.lower()
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device path")
+@pytest.mark.parametrize("igamma", [1, 2])
+def test_discrete_green_decks_are_accepted(tmp_path, igamma):
+    """IGAMMA 1 (central differences) and 2 (rotated scheme) pass the deck checks."""
+    fft = decks.write_case(decks.case_c1(nsteps=2), tmp_path)
+    fft.write_text(fft.read_text().replace("2.0 0            XC0", f"2.0 {igamma}            XC0", 1))
+    rc, msg = _open(fft)
+    assert rc == -6 and "CUDA" in msg
 
 
 def test_missing_deck_is_refused(tmp_path):

@@ -137,3 +137,38 @@ def test_substep_rollback_parity(tmp_path):
     assert len(rg) > 4  # substeps were taken
     for f in ("sg", "velgrad", "gamdot"):
         assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
+
+
+@pytest.mark.parametrize("igamma", [1, 2])
+def test_discrete_green_operator_parity(tmp_path, igamma):
+    """IGAMMA 1 (central differences, four projections) and 2 (rotated scheme): the Green
+    operator is tabulated once per increment; both with and without the modified augmented
+    Lagrangian.
+
+    On an even grid the node coordinates are compared loosely: the reference integrates the
+    strain rate with the same discrete derivative, whose symbol sin(xi) (IGAMMA 1) or the
+    rotated-scheme factor (IGAMMA 2, where two Nyquist planes meet) is ~1e-16 at Nyquist
+    points without being zero, so it divides there by ~1e-32 and the node positions carry
+    FFT rounding amplified ~1e16 times, different for every FFT implementation.  The odd grid
+    of the next test has no Nyquist points and checks the integration at the strict bound."""
+    case = decks.case_c2(nsteps=3, n=12, ngrains=12)
+    case.processes[0].igamma = igamma
+    fft = _case(tmp_path, case)
+    for modal in (0, 1):
+        g, o, rg, ro, dg, do = parity.run_both(fft, 3, mix=1, modal=modal)
+        parity.assert_rows_match(rg, ro, dg, do)
+        for f in ("sg", "velgrad", "gamdot", "disgradsym", "defgrad", "crss"):
+            assert parity.field_rel_err(g, o, f) <= parity.RTOL, (modal, f)
+        assert parity.field_rel_err(g, o, "xnode") <= 1e-4, modal
+
+
+@pytest.mark.parametrize("igamma", [1, 2])
+def test_discrete_green_operator_odd_grid_parity(tmp_path, igamma):
+    """15^3 (radix 3 and 5, no Nyquist points): every field, node coordinates included, at 1e-8."""
+    case = decks.case_c2(nsteps=2, n=15, ngrains=12)
+    case.processes[0].igamma = igamma
+    fft = _case(tmp_path, case)
+    g, o, rg, ro, dg, do = parity.run_both(fft, 2)
+    parity.assert_rows_match(rg, ro, dg, do)
+    for f in FIELDS:
+        assert parity.field_rel_err(g, o, f) <= parity.RTOL, f
