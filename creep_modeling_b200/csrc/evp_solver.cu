@@ -117,7 +117,7 @@ public:
     double gpu_ms = 0.0;
     std::time_t start = 0;
     std::string outdir;
-    double last_results[53] = {}, last_diag[44] = {};
+    double last_results[51] = {}, last_diag[44] = {};
     std::vector<double> snap_dsim, snap_scau;
     bool has_thermo = false;
     std::vector<double> eth_soa;  // host staging of the thermal eigenstrain upload (kept until the copy completes)
@@ -932,9 +932,9 @@ public:
         std::fputs(line.c_str(), f);
         std::fclose(f);
         line.clear();
-        for (int q = 0; q < 53; q++) {
+        for (int q = 0; q < 51; q++) {
             line += (q < 3) ? std::to_string((long long)R[q]) : g0(R[q]);
-            line += (q == 52) ? '\n' : ',';
+            line += (q == 50) ? '\n' : ',';
         }
         f = std::fopen(csv_path("results.csv").c_str(), "a");
         if (!f) throw SolveError("write_results: failed to open results.csv for append", -5);
@@ -1214,9 +1214,9 @@ int evp_get_field(evp_solve* h, const char* name, double* host_out, long long ca
     return 0;
 }
 
-int evp_last_rows(evp_solve* h, double* r53, double* d44) {
+int evp_last_rows(evp_solve* h, double* r51, double* d44) {
     if (!h) return fail("evp_last_rows: null handle", -7);
-    if (r53) std::memcpy(r53, h->s.last_results, sizeof(h->s.last_results));
+    if (r51) std::memcpy(r51, h->s.last_results, sizeof(h->s.last_results));
     if (d44) std::memcpy(d44, h->s.last_diag, sizeof(h->s.last_diag));
     return 0;
 }

@@ -75,7 +75,7 @@ class Solve:
         return rows
 
     def rows(self):
-        r = np.zeros(53)
+        r = np.zeros(51)
         d = np.zeros(44)
         _lib.load().evp_last_rows(self._h, r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                   d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))

@@ -66,9 +66,9 @@ int evp_advance(evp_solve* s, int nmacro, int* done);
  * wgtc, gacumgr, epvm, xnode.  *written = number of doubles copied. */
 int evp_get_field(evp_solve* s, const char* name, double* host_out, long long capacity, long long* written);
 
-/* Last results.csv row (53 values, IO_functions.f90:1264-1271 order) and
+/* Last results.csv row (51 values, IO_functions.f90:1264-1271 order) and
  * diagnostics.csv row (44 values, types.f90:787-798 order). */
-int evp_last_rows(evp_solve* s, double* results53, double* diag44);
+int evp_last_rows(evp_solve* s, double* results51, double* diag44);
 int evp_stats(evp_solve* s, evp_report* out);
 int evp_close(evp_solve* s);
 

@@ -109,7 +109,7 @@ class OracleSolve:
         return buf[:n].copy()
 
     def rows(self):
-        r = np.zeros(53)
+        r = np.zeros(51)
         d = np.zeros(44)
         lib().oracle_last_rows(self._h, _p(r), _p(d))
         return r, d

@@ -199,7 +199,7 @@ struct Oracle {
     // ---- outputs
     std::string outdir;
     bool write_files = false, verbose = false;
-    double last_results[53] = {}, last_diag[44] = {};
+    double last_results[51] = {}, last_diag[44] = {};
 
     long vidx(int i, int j, int k) const { return i + (long)n1 * (j + (long)n2 * k); }
     Process& P() { return process[ipr - 1]; }
@@ -1519,10 +1519,10 @@ struct Oracle {
         std::fclose(f);
         f = std::fopen(csv("results.csv").c_str(), "a");
         if (!f) throw SolveError("write_results: failed to open results.csv for append", -5);
-        for (int q = 0; q < 53; q++) {
+        for (int q = 0; q < 51; q++) {
             if (q < 3) std::fprintf(f, "%d", (int)R[q]);
             else std::fprintf(f, "%s", fmt_g0(R[q]).c_str());
-            std::fputc(q == 52 ? '\n' : ',', f);
+            std::fputc(q == 50 ? '\n' : ',', f);
         }
         std::fclose(f);
     }
@@ -1997,8 +1997,8 @@ int oracle_advance(oracle_solve* s, int nmacro) {
 
 long oracle_get_field(oracle_solve* s, const char* name, double* out, long n) { return s->o.get_field(name, out, n); }
 
-int oracle_last_rows(oracle_solve* s, double* r53, double* d44) {
-    if (r53) std::memcpy(r53, s->o.last_results, sizeof(s->o.last_results));
+int oracle_last_rows(oracle_solve* s, double* r51, double* d44) {
+    if (r51) std::memcpy(r51, s->o.last_results, sizeof(s->o.last_results));
     if (d44) std::memcpy(d44, s->o.last_diag, sizeof(s->o.last_diag));
     return 0;
 }

@@ -100,3 +100,22 @@ def test_micro_file_grammar(tmp_path):
     f = lines[0].split()
     assert len(f) == 8 and f[3:6] == ["1", "1", "1"]
     assert 1 <= int(f[6]) <= 5 and f[7] == "1"
+
+
+def test_results_csv_rows_match_header(oracle_lib, tmp_path):
+    """results.csv and diagnostics.csv rows have exactly the header's fields (51 and 44,
+    IO_functions.f90:1264-1296, types.f90:787-834), so loaders that select columns by
+    name (the reference's SimResults.load) read the right values."""
+    import pandas as pd
+
+    c = decks.case_c1(nsteps=1)
+    c.n = 8
+    c.ngrains = 6
+    fft = decks.write_case(c, tmp_path / "d")
+    assert oracle_lib.run_file(fft, tmp_path / "out") == 0
+    for name, nf in (("results.csv", 51), ("diagnostics.csv", 44)):
+        lines = (tmp_path / "out" / name).read_text().splitlines()
+        assert [len(r.split(",")) for r in lines] == [nf] * len(lines), name
+    df = pd.read_csv(tmp_path / "out" / "results.csv")
+    assert list(df["macrostep"]) == [1] and df["iter"][0] > 1
+    assert abs(df["sav33"][0] - 150.0) < 1.0

@@ -73,3 +73,6 @@ def test_written_files_match_the_oracle(tmp_path, oracle_lib):
     parity.assert_rows_match(rg, ro, dg, do)
     assert (out_g / "results.csv").read_text().splitlines()[0] == (out_o / "results.csv").read_text().splitlines()[0]
     assert (out_g / "diagnostics.csv").read_text().splitlines()[0] == (out_o / "diagnostics.csv").read_text().splitlines()[0]
+    for name in ("results.csv", "diagnostics.csv"):  # every row has the header's field count (pandas reads by name)
+        lines = (out_g / name).read_text().splitlines()
+        assert {len(r.split(",")) for r in lines} == {len(lines[0].split(","))}, name
