@@ -302,6 +302,52 @@ void read_elastic_file(const std::string& path, PhaseData& ph) {
 
 }  // namespace
 
+// Initial displacement file of IDISPINI (init_defgrad, IO_functions.f90:815-880): records
+// "i j k u1 u2 u3" in loop order (the indices are read and ignored).  IDISPINI 1: one per cell
+// centre, nodes by cell2node_tensor1 (various_functions.f90:2652-2691, x wrapped with n1);
+// IDISPINI 2: one per node ((n1+1)(n2+1) x n3node), cells take their lower-corner node.
+static void read_dispini(Deck& d, const std::string& path) {
+    if (d.idispini != 1 && d.idispini != 2) throw DeckError("idispini must be 0, 1 or 2", -1);
+    Records f(path);
+    const int n1 = d.n1, n2 = d.n2, n3 = d.n3, nn3 = (n3 == 1) ? 1 : n3 + 1;
+    const long long N = d.nvox();
+    const long long nn1 = n1 + 1, nn2 = n2 + 1;
+    auto node = [&](long long i, long long j, long long k) { return 3 * (i + nn1 * (j + nn2 * k)); };
+    d.dispini.assign(3 * (size_t)N, 0.0);
+    d.dispini_node.assign(3 * (size_t)(nn1 * nn2 * nn3), 0.0);
+    if (d.idispini == 1) {
+        for (long long v = 0; v < N; v++) {
+            auto t = f.reals(6);
+            for (int l = 0; l < 3; l++) d.dispini[3 * v + l] = t[3 + l];
+        }
+        auto cell = [&](long long i, long long j, long long k, int l) { return d.dispini[3 * (i + n1 * (j + (long long)n2 * k)) + l]; };
+        for (long long k = 0; k < nn3; k++) {
+            const long long k1 = (k + n3 - 1) % n3, k2 = k % n3;
+            for (long long j = 0; j < nn2; j++) {
+                const long long j1 = (j + n2 - 1) % n2, j2 = j % n2;
+                for (long long i = 0; i < nn1; i++) {
+                    const long long i1 = (i + n1 - 1) % n1, i2 = i % n1;
+                    for (int l = 0; l < 3; l++)
+                        d.dispini_node[node(i, j, k) + l] =
+                            (cell(i2, j2, k2, l) + cell(i1, j2, k2, l) + cell(i2, j1, k2, l) + cell(i2, j2, k1, l) +
+                             cell(i1, j1, k2, l) + cell(i1, j2, k1, l) + cell(i2, j1, k1, l) + cell(i1, j1, k1, l)) * 0.125;
+                }
+            }
+        }
+    } else {
+        for (long long k = 0; k < nn3; k++)
+            for (long long j = 0; j < nn2; j++)
+                for (long long i = 0; i < nn1; i++) {
+                    auto t = f.reals(6);
+                    for (int l = 0; l < 3; l++) d.dispini_node[node(i, j, k) + l] = t[3 + l];
+                }
+        for (long long v = 0; v < N; v++) {
+            const long long i = v % n1, j = (v / n1) % n2, k = v / ((long long)n1 * n2);
+            for (int l = 0; l < 3; l++) d.dispini[3 * v + l] = d.dispini_node[node(i, j, k) + l];
+        }
+    }
+}
+
 Deck parse_deck(const std::string& fft_in) {
     Deck d;
     Records r(fft_in);
@@ -377,7 +423,7 @@ Deck parse_deck(const std::string& fft_in) {
     d.complgas = r.reals(1)[0];
     r.line();
     d.idispini = (int)r.ints(1)[0];
-    if (d.idispini > 0) throw DeckError("IDISPINI > 0 (initial displacement field) is not supported", -2);
+    if (d.idispini > 0) read_dispini(d, strip(r.line()));
     d.nproc = (int)r.ints(1)[0];
     if (d.nproc < 1) throw DeckError("cannot have less than one processes", -1);
     d.process.assign(d.nproc, ProcessData());

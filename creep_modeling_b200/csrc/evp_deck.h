@@ -48,6 +48,9 @@ struct Deck {
     std::vector<int> grain, phase_id;
     std::vector<double> hp_shift;  // Hall-Petch tau0 shift per voxel (IO_functions.f90:107-199)
     std::vector<double> eth;       // 9 per voxel (only when some process has ithermo=1)
+    // IDISPINI 1, 2 (IO_functions.f90:815-936): initial displacement at the cell centres (3 per voxel)
+    // and at the nodes (3 per node, node index i + (n1+1)(j + (n2+1) k), k < n3node)
+    std::vector<double> dispini, dispini_node;
     bool has_gas = false;
     long long nvox() const { return (long long)n1 * n2 * n3; }
 };

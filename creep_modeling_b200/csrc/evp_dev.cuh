@@ -39,12 +39,13 @@ enum : int {
     OFF_DIAG = 224,   // 24+ diagnostics reductions
     OFF_C0 = 272,     // 72 macro tangent sums (b-basis dsg/de, PK1 tangent)
     OFF_KIN = 392,    // 4   kinematic increment maxima
+    OFF_DISP = 344,   // 30  init_defgrad sums (F^-1 w J all/solid/gas, w J solid/gas, J w)
     OFF_DC = 400,     // 18  DC of the grid-update spectrum (complex x 9)
     OFF_G0 = 420,     // 81  real-space Green operator at the origin
     RED_OUT_SIZE = 512
 };
 
-enum : int { CNT_SGAVG = 0, CNT_XINV, CNT_CORR, CNT_NEWTON, CNT_INIT, CNT_UPD1, CNT_UPD2, CNT_UPD3, CNT_DIAG, CNT_DIAG2, CNT_C0, CNT_KIN, CNT_G0, CNT_N };
+enum : int { CNT_SGAVG = 0, CNT_XINV, CNT_CORR, CNT_NEWTON, CNT_INIT, CNT_UPD1, CNT_UPD2, CNT_UPD3, CNT_DIAG, CNT_DIAG2, CNT_C0, CNT_KIN, CNT_G0, CNT_DISP, CNT_N };
 
 struct FftPlan1D {
     int n;
@@ -81,6 +82,7 @@ struct Dev {
     // goper[c * (n1h n2 n3) + (k3 n2 + j) n1h + kx]; gtab = 1 while the current process uses it
     double* goper;
     int gtab;
+    double* Fini;  // initial deformation gradient (IDISPINI 1, 2 only; null: identity)
     // reductions
     double *partials, *red;
     unsigned int *counters;
@@ -115,8 +117,13 @@ struct Upd3Params {
 };
 
 // ---- launch wrappers (stream-ordered)
+// keepF: F, F^-1, det F and the unscaled weights w J were set by launch_dispini; the weights
+// are divided by detFavg here (IO_functions.f90:934) and weight the start-up tangent sum
 void launch_init(const Dev& d, const double* euler, const int* grain, const double* hp, const double* udot9, const double* u6t,
-                 cudaStream_t st);
+                 int keepF, double detFavg, cudaStream_t st);
+// init_defgrad per voxel (IO_functions.f90:893-921): F = grad(u) + diag(delt) from the gradient
+// field (component 3m + l = d u_l / d x_m), F_ini = F, det F, F^-1, w J and the OFF_DISP sums
+void launch_dispini(const Dev& d, const double* grad, double delt, cudaStream_t st);
 void launch_sgavg(const Dev& d, cudaStream_t st);
 void launch_prologue(const Dev& d, const double* c0, const double* goperr0, int do_schmid, int modal, cudaStream_t st);
 void launch_goperr0(const Dev& d, const double* c0, const double* s0, int igamma, cudaStream_t st);
@@ -145,6 +152,10 @@ void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
 void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st, int prec = 0);
 void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st, int prec = 0);
 void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st);
+// gradient_tensor1 (various_functions.f90:56-112) of a vector field given as 9 real fields with
+// component 3m + l = u_l: out component 3m + l = d u_l / d x_m (spectral derivative ideriv)
+void launch_gradient(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* u9,
+                     double* out, int ideriv, cudaStream_t st);
 void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st, int prec = 0);
 
 }  // namespace evp

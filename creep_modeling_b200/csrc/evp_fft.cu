@@ -493,6 +493,60 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
     }
 }
 
+// ---------------------------------------------------------------- z fused with the spectral gradient (IDISPINI start-up)
+// The spectrum holds 9 components with component 3m + l = u_l; each is multiplied by the
+// derivative symbol of direction m (ideriv 1: i sin(xi), 2: the rotated-scheme kmod, zero at the
+// point where all three Nyquist planes meet), so the inverse gives d u_l / d x_m
+// (gradient_tensor1, various_functions.f90:56-112).
+template <int RS>
+__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_grad(Dev d, FftPlan1D pl, int T, int ideriv) {
+    extern __shared__ double2 s[];
+    const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
+    const int kx0 = blockIdx.x * T, j = blockIdx.y;
+    const int P = 9 * T;
+    const long long plane = (long long)n2 * n1h;
+    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+        s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    fft_run<false, RS, double2>(s, P, P, pl, d.tw3);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < T * n3; idx += blockDim.x) {
+        const int t = idx % T, k3 = idx / T, kx = kx0 + t;
+        if (kx >= n1h) continue;
+        double2* q = s + k3 * P + t;
+        const double xi[3] = {xi_of(kx, n1), xi_of(j, n2), (n3 == 1) ? 0.0 : xi_of(k3, n3)};
+        double2 km[3];
+        if (ideriv == 2) {
+            double2 b = make_double2(0.0, 0.25);
+            for (int l = 0; l < 3; l++) {
+                double sn, cs;
+                sincos(xi[l], &sn, &cs);
+                b = cmul(b, make_double2(1.0 + cs, sn));
+            }
+            for (int l = 0; l < 3; l++) { const double tn = tan(xi[l] / 2.0); km[l] = make_double2(tn * b.x, tn * b.y); }
+        } else {
+            for (int l = 0; l < 3; l++) km[l] = make_double2(0.0, (ideriv == 0) ? xi[l] : sin(xi[l]));
+        }
+        const bool zero = ideriv == 2 && (n1 % 2 == 0 && kx == n1 / 2) && (n2 % 2 == 0 && j == n2 / 2) &&
+                          (n3 % 2 == 0 && k3 == n3 / 2 && n3 > 1);
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+            for (int l = 0; l < 3; l++) {
+                const int c = 3 * m + l;
+                q[c * T] = zero ? make_double2(0.0, 0.0) : cmul(q[c * T], km[m]);
+            }
+    }
+    __syncthreads();
+    fft_run<true, RS, double2>(s, P, P, pl, d.tw3);
+    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+        if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
+    }
+}
+
 // ---------------------------------------------------------------- x inverse (C2R)
 template <int RS, class CT>
 __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
@@ -826,6 +880,39 @@ static void z_integ_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream
 void launch_fft_z_integ(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
     if (plan_pow2(pl)) z_integ_rs<0>(d, pl, ideriv, st);
     else z_integ_rs<1>(d, pl, ideriv, st);
+}
+
+template <int RS>
+static void z_grad_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
+    static const int mx = kernel_max_threads((const void*)k_fft_z_grad<RS>);
+    int thr = 0;
+    const int T = choose_tile((const void*)k_fft_z_grad<RS>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+                              [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
+                              [&](int t) { return (size_t)9 * t * d.n3 * sizeof(double2); }, thr);
+    dim3 grid((d.n1h + T - 1) / T, d.n2);
+    const size_t smem = (size_t)9 * T * d.n3 * sizeof(double2);
+    k_fft_z_grad<RS><<<grid, thr, smem, st>>>(d, pl, T, ideriv);
+}
+template <int RS>
+static void gradient_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* u9,
+                        double* out, int ideriv, cudaStream_t st) {
+    static const int mx = std::min(kernel_max_threads((const void*)k_green_x_fwd<RS>), kernel_max_threads((const void*)k_green_x_inv<RS>));
+    int thr = 0;
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, fft_maxb<RS>(), 256, mx, thr);
+    const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
+    const int grid = (npairs + G - 1) / G;
+    const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
+    k_green_x_fwd<RS><<<grid, thr, smem, st>>>(d, pl1, G, u9);
+    launch_fft_y(d, pl2, 9, false, st, 0);
+    if (plan_pow2(pl3)) z_grad_rs<0>(d, pl3, ideriv, st);
+    else z_grad_rs<1>(d, pl3, ideriv, st);
+    launch_fft_y(d, pl2, 9, true, st, 0);
+    k_green_x_inv<RS><<<grid, thr, smem, st>>>(d, pl1, G, out);
+}
+void launch_gradient(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* u9,
+                     double* out, int ideriv, cudaStream_t st) {
+    if (plan_pow2(pl1)) gradient_rs<0>(d, pl1, pl2, pl3, u9, out, ideriv, st);
+    else gradient_rs<1>(d, pl1, pl2, pl3, u9, out, ideriv, st);
 }
 template <int RS, class CT>
 static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {

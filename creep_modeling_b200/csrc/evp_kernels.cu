@@ -137,6 +137,8 @@ __device__ __forceinline__ double powabs(double x, double e, int int_exp) {
 struct InitParams {
     double udot[9];
     double u6t[6];  // b6(udot) * tdot of process 1
+    int keepF;       // F, F^-1, det F and w J come from k_dispini
+    double detFavg;  // sum of w J (divides the weights when keepF)
 };
 
 __global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict__ euler, const int* __restrict__ grain,
@@ -150,10 +152,15 @@ __global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict
         const PhaseDev& ph = d.ph[p];
         double I9[9];
         eye9(I9);
-        st9(d.F, N, v, I9); st9(d.Fe, N, v, I9); st9(d.Fp, N, v, I9); st9(d.Finv, N, v, I9);
+        if (!ip.keepF) {
+            st9(d.F, N, v, I9);
+            st9(d.Finv, N, v, I9);
+            d.detF[v] = 1.0;
+        }
+        st9(d.Fe, N, v, I9); st9(d.Fp, N, v, I9);
         st9(d.Finc, N, v, I9); st9(d.Feinc, N, v, I9);
-        d.detF[v] = 1.0;
-        d.wgtc[v] = d.wgt;
+        const double w = ip.keepF ? d.wgtc[v] / ip.detFavg : d.wgt;  // wgtc (IO_functions.f90:917, 934)
+        d.wgtc[v] = w;
         d.epvm[v] = 0.0;
         d.gacumgr[v] = 0.0;
         st9(d.velgrad, N, v, ip.udot);
@@ -182,7 +189,7 @@ __global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict
         double c4[81], cg66[36];
         rotate4(ag, ph.C, c4);
         t4_to_b66(c4, cg66);
-        for (int c = 0; c < 36; c++) sums[c] += cg66[c] * d.wgt;
+        for (int c = 0; c < 36; c++) sums[c] += cg66[c] * w;
         double sg6[6], s6[6];
         for (int i = 0; i < 6; i++) {
             double s = 0.0;
@@ -210,11 +217,50 @@ __global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict
 }
 
 void launch_init(const Dev& d, const double* euler, const int* grain, const double* hp, const double* udot9, const double* u6t,
-                 cudaStream_t st) {
+                 int keepF, double detFavg, cudaStream_t st) {
     InitParams ip;
     for (int c = 0; c < 9; c++) ip.udot[c] = udot9[c];
     for (int c = 0; c < 6; c++) ip.u6t[c] = u6t[c];
+    ip.keepF = keepF;
+    ip.detFavg = detFavg;
     k_init<<<d.grid, kBlock, 0, st>>>(d, euler, grain, hp, ip);
+}
+
+// ---------------------------------------------------------------- k_dispini
+// init_defgrad per voxel (IO_functions.f90:893-921).  Sums, in OFF_DISP order: F^-1 w J over all
+// voxels (9), the solid ones (9), the gas ones (9); w J over solid and gas voxels; J w.
+__global__ void __launch_bounds__(kBlock) k_dispini(Dev d, const double* __restrict__ grad, double delt) {
+    const long long N = d.N;
+    double sums[30];
+#pragma unroll
+    for (int c = 0; c < 30; c++) sums[c] = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        double F[9], Fi[9];
+        for (int l = 0; l < 3; l++)
+            for (int m = 0; m < 3; m++) F[3 * l + m] = grad[(size_t)(3 * m + l) * N + v] + (l == m ? delt : 0.0);
+        const double J = det33(F);
+        if (inv3u(F, Fi) != 0) set_err(d.err, 1);
+        st9(d.F, N, v, F);
+        st9(d.Fini, N, v, F);
+        st9(d.Finv, N, v, Fi);
+        d.detF[v] = J;
+        d.wgtc[v] = d.wgt * J;
+        const int gas = d.gas[v];
+#pragma unroll
+        for (int c = 0; c < 9; c++) {
+            const double t = Fi[c] * d.wgt * J;
+            sums[c] += t;
+            sums[9 + c] += gas ? 0.0 : t;
+            sums[18 + c] += gas ? t : 0.0;
+        }
+        sums[27] += gas ? 0.0 : d.wgt * J;
+        sums[28] += gas ? d.wgt * J : 0.0;
+        sums[29] += J * d.wgt;
+    }
+    reduce_store<30, 0>(sums, nullptr, d.partials, d.red + OFF_DISP, d.counters + CNT_DISP);
+}
+void launch_dispini(const Dev& d, const double* grad, double delt, cudaStream_t st) {
+    k_dispini<<<d.grid, kBlock, 0, st>>>(d, grad, delt);
 }
 
 // ---------------------------------------------------------------- k_sgavg
@@ -1745,13 +1791,21 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
         double Finc[9], Feinc[9];
         ld9(d.Finc, N, v, Finc);
         if (!gas) {
-            // update_elstic_defgrad (various_functions.f90:2285-2324), Fini = I
+            // update_elstic_defgrad (various_functions.f90:2285-2324): Fe = F (Fp Fini)^-1, Fini = I
+            // unless an initial displacement field was given
             const PhaseDev& ph = d.ph[d.phase[v]];
             double Fe[9], Feo[9], Fp[9], Fpi[9], F[9];
             ld9(d.Fe, N, v, Fe);
             if (inv3u(Fe, Feo) != 0) set_err(d.err, 1);
             ld9(d.Fp, N, v, Fp);
-            if (inv3u(Fp, Fpi) != 0) set_err(d.err, 1);
+            if (d.Fini) {
+                double Fi0[9], FpFi[9];
+                ld9(d.Fini, N, v, Fi0);
+                mm3(Fp, Fi0, FpFi);
+                if (inv3u(FpFi, Fpi) != 0) set_err(d.err, 1);
+            } else if (inv3u(Fp, Fpi) != 0) {
+                set_err(d.err, 1);
+            }
             ld9(d.F, N, v, F);
             mm3(F, Fpi, Fe);
             mm3(Fe, Feo, Feinc);

@@ -58,7 +58,7 @@ bool deck_grid(const std::string& fft, int& n1, int& n2, int& n3) {
 // point), the node coordinates and fixed buffers.
 unsigned long long footprint(int n1, int n2, int n3) {
     const unsigned long long N = (unsigned long long)n1 * n2 * n3;
-    const unsigned long long per_voxel = 660ull * 8ull;
+    const unsigned long long per_voxel = 669ull * 8ull;
     const unsigned long long spec = 9ull * 16ull * (unsigned long long)(n1 / 2 + 1) * n2 * n3;
     const unsigned long long goper = 81ull * 8ull * (unsigned long long)(n1 / 2 + 1) * n2 * n3;
     const unsigned long long nodes = 3ull * 8ull * (n1 + 1ull) * (n2 + 1ull) * (n3 + 1ull);

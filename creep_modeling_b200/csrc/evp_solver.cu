@@ -295,6 +295,7 @@ public:
         }
         d.tw1 = dalloc<double2>(dk.n1); d.tw2 = dalloc<double2>(dk.n2); d.tw3 = dalloc<double2>(dk.n3);
         d.dv3 = dalloc<double>(3 * N);
+        d.Fini = dk.idispini > 0 ? dalloc<double>(9 * N) : nullptr;
         d.xnode = dalloc<double>(3 * (size_t)(dk.n1 + 1) * (dk.n2 + 1) * d.n3node);
         // block partials: voxel kernels (<= 1184 blocks x 117 sums), Newton (<= 3552 x 14), and the
         // x inverse pass (one block per <= 1 pair of rows x 9 sums)
@@ -367,6 +368,32 @@ public:
         d.nph = dk.nph;
     }
 
+    // init_defgrad (IO_functions.f90:815-936): F = grad(u) + diag(delt) (delt forced to 4), the
+    // spectral gradient with ideriv = IDISPINI; the macroscopic weights and inverse averages.
+    // velgradold and dvr are scratch here (k_init clears both afterwards).
+    void init_defgrad(double& detFavg) {
+        const long long N = d.N;
+        std::vector<double> u9(9 * (size_t)N);
+        for (int m = 0; m < 3; m++)
+            for (int l = 0; l < 3; l++)
+                for (long long v = 0; v < N; v++) u9[(size_t)(3 * m + l) * N + v] = dk.dispini[3 * (size_t)v + l];
+        h2d_copy(d.velgradold, u9.data(), u9.size() * sizeof(double));
+        K("k_gradient", [&] { launch_gradient(d, pl1, pl2, pl3, d.velgradold, d.dvr, dk.idispini, st); });
+        K("k_dispini", [&] { launch_dispini(d, d.dvr, 4.0, st); });
+        fetch_red();
+        const double* S = h_red + OFF_DISP;
+        detFavg = S[29];
+        wphcsol = S[27] / detFavg;
+        wphcgas = S[28] / detFavg;
+        for (int c = 0; c < 9; c++) {
+            const double id = (c % 4 == 0) ? 1.0 : 0.0;
+            defgradavg[c] = 4.0 * id;  // diag(delt)
+            dinvc[c] = S[c] / detFavg;
+            dinvcs[c] = S[9 + c] / detFavg / wphcsol;
+            dinvcg[c] = (wphcgas > 0.0) ? S[18 + c] / detFavg / wphcgas : id;
+        }
+    }
+
     void upload_and_init() {
         const long long N = d.N;
         std::vector<uint8_t> gas(N), phs(N);
@@ -409,13 +436,17 @@ public:
                         xn[p + 1] = (double)(j + 1) - 0.5;
                         xn[p + 2] = (nn3 == 1) ? 0.0 : (double)(k + 1) - 0.5;
                     }
+            if (dk.idispini > 0)  // xnode + dispini_node (IO_functions.f90:885); same node layout
+                for (size_t q = 0; q < xn.size(); q++) xn[q] = xn[q] + dk.dispini_node[q];
             h2d_copy(d.xnode, xn.data(), xn.size() * sizeof(double));
         }
+        double detFavg = 1.0;
+        if (dk.idispini > 0) init_defgrad(detFavg);
         const ProcessData& p1 = dk.process[0];
         double u6[6], u6t[6];
         t2_to_b6(p1.udot, u6);
         for (int c = 0; c < 6; c++) u6t[c] = u6[c] * p1.tdot;
-        launch_init(d, d_eul, d_gr, d_hp, p1.udot, u6t, st);
+        launch_init(d, d_eul, d_gr, d_hp, p1.udot, u6t, dk.idispini > 0 ? 1 : 0, detFavg, st);
         CK(cudaGetLastError());
         fetch_red();
         // release the start-up staging buffers

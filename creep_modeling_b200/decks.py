@@ -271,7 +271,8 @@ def _process_block(p: Loading) -> str:
 
 
 def write_fft_in(path: Path, n, micro: Path, cupl2: Path, cuel: Path, processes: list[Loading],
-                 phase2: tuple[int, Path, Path] | None = None, complgas: float = 0.0) -> None:
+                 phase2: tuple[int, Path, Path] | None = None, complgas: float = 0.0,
+                 dispini: tuple[int, Path] | None = None) -> None:
     n1, n2, n3 = (n, n, n) if isinstance(n, int) else n
     nph = 1 if phase2 is None else 2
     txt = (f"{nph}                      number of phases (nph)\n"
@@ -293,7 +294,8 @@ def write_fft_in(path: Path, n, micro: Path, cupl2: Path, cuel: Path, processes:
             "0 200                  ires,imicrosave\n"
             f"{complgas}                   complgas (% of stiffness)\n"
             "* initial displacement field\n"
-            "0                      IDISPINI (if idispini=1, next line is filedispl)\n"
+            + ("0                      IDISPINI (if idispini=1, next line is filedispl)\n" if dispini is None else
+               f"{dispini[0]}                      IDISPINI (if idispini=1, next line is filedispl)\n{dispini[1]}\n") +
             f"{len(processes)}                      number of processes (nproc)\n")
     for p in processes:
         txt += _process_block(p)
@@ -312,6 +314,8 @@ class Case:
     phase2_gas: bool = False  # the second phase as gas (igas = 1) instead of the stiff elastic phase
     complgas: float = 0.0
     thermo_eigenstrain: float = 0.0  # > 0: per-grain thermal eigenstrain of this size (ITHERMO = 1)
+    dispini: int = 0  # 1: initial displacement at cell centres, 2: at nodes (IDISPINI)
+    dispini_amp: float = 0.05  # amplitude of that displacement field, in voxels
 
 
 def case_c1(nsteps: int = 100) -> Case:
@@ -352,10 +356,38 @@ def write_case(case: Case, root: Path, micro_cache: dict | None = None) -> Path:
     if case.thermo_eigenstrain > 0.0:
         write_thermo(root / "thermo.txt", case.ngrains, case.thermo_eigenstrain, case.seed)
         processes = [dataclasses.replace(p, thermo_file=str(root / "thermo.txt")) for p in processes]
+    dispini = None
+    if case.dispini:
+        write_dispini(root / "disp.txt", case.n, case.dispini, case.dispini_amp, case.seed)
+        dispini = (case.dispini, root / "disp.txt")
     fft = root / "fft.in"
     write_fft_in(fft, case.n, micro, root / "cupl2.sx", root / "cuel.sx", processes, phase2=phase2,
-                 complgas=case.complgas)
+                 complgas=case.complgas, dispini=dispini)
     return fft
+
+
+def write_dispini(path: Path, n, kind: int, amp: float, seed: int) -> None:
+    """Initial displacement file read after IDISPINI (IO_functions.f90:850-880): one line
+    ``i j k u1 u2 u3`` per cell centre (kind 1, i fastest) or per node (kind 2, (n+1) per axis,
+    one z plane when n3 = 1).  The field is a smooth periodic one: a sum of three seeded
+    sine modes of amplitude ``amp`` voxels per component."""
+    n1, n2, n3 = (n, n, n) if isinstance(n, int) else n
+    rng = np.random.default_rng([seed, 11])
+    kvec = rng.integers(1, 3, size=(3, 3, 3))  # component, mode, axis
+    phase = rng.uniform(0.0, 2.0 * np.pi, size=(3, 3))
+    off = 0.5 if kind == 1 else 0.0  # cell centres sit half a voxel from the nodes
+    m1, m2 = (n1, n2) if kind == 1 else (n1 + 1, n2 + 1)
+    m3 = n3 if kind == 1 else (1 if n3 == 1 else n3 + 1)
+    k, j, i = np.meshgrid(np.arange(m3), np.arange(m2), np.arange(m1), indexing="ij")
+    x = (i + off) / n1, (j + off) / n2, (k + off) / n3
+    u = np.zeros((3,) + i.shape)
+    for c in range(3):
+        for mo in range(3):
+            arg = 2 * np.pi * sum(kvec[c, mo, a] * x[a] for a in range(3)) + phase[c, mo]
+            u[c] += amp / 3.0 * np.sin(arg)
+    lines = [f"{a + 1} {b + 1} {cc + 1} {u0:.15e} {u1:.15e} {u2:.15e}"
+             for cc, b, a, u0, u1, u2 in zip(k.ravel(), j.ravel(), i.ravel(), u[0].ravel(), u[1].ravel(), u[2].ravel())]
+    Path(path).write_text("\n".join(lines) + "\n")
 
 
 def write_thermo(path: Path, ngrains: int, size: float, seed: int) -> None:

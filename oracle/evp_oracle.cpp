@@ -426,7 +426,12 @@ struct Oracle {
         complgas = r.read_reals(1)[0];
         r.read_line();
         idispini = (int)r.read_ints(1)[0];
-        if (idispini > 0) throw DeckError("IDISPINI > 0 (initial displacement field) is not supported");
+        std::string filedispl;
+        if (idispini > 0) {
+            if (idispini > 2) throw DeckError("idispini must be 0, 1 or 2");
+            filedispl = trim(r.read_line());
+            init_defgrad(filedispl);
+        }
         for (long v = 0; v < N; v++) {
             Voxel& x = vox[v];
             x.gacumgr = 0.0;
@@ -547,8 +552,126 @@ struct Oracle {
             if (vox[v].gas) wphgas += wgt;
             if (!vox[v].gas) wphsol += wgt;
         }
-        wphcgas = wphgas;
-        wphcsol = wphsol;
+        if (idispini == 0) {
+            wphcgas = wphgas;
+            wphcsol = wphsol;
+        }
+    }
+
+    // ------------------------------------------------------------ init_defgrad (IO_functions.f90:815-936)
+    // Initial displacement field: cell centres (IDISPINI 1, nodes by cell2node_tensor1) or nodes
+    // (IDISPINI 2, cells = the lower-corner nodes); F = grad u + diag(delt) with delt = 4 as forced
+    // at IO_functions.f90:62-66; gradient_tensor1 (various_functions.f90:56-112) with ideriv 1 or 2.
+    void init_defgrad(const std::string& fdisp) {
+        const long nn1 = n1 + 1, nn2 = n2 + 1, nn3 = n3 + 1;
+        std::vector<double> u(3 * N), un(3 * nn1 * nn2 * nn3, 0.0);
+        auto node = [&](long i, long j, long k) { return 3 * (i + nn1 * (j + nn2 * k)); };
+        RecordReader f(fdisp);
+        int ideriv;
+        if (idispini == 1) {
+            for (long v = 0; v < N; v++) {
+                auto t = f.read_reals(6);
+                for (int l = 0; l < 3; l++) u[3 * v + l] = t[3 + l];
+            }
+            // cell2node_tensor1 (various_functions.f90:2652-2691), x wrapped with n1
+            for (long k = 1; k <= n3 + 1; k++) {
+                long k1 = k - 1, k2 = k;
+                if (k1 == 0) k1 = n3;
+                if (k2 == n3 + 1) k2 = 1;
+                for (long j = 1; j <= n2 + 1; j++) {
+                    long j1 = j - 1, j2 = j;
+                    if (j1 == 0) j1 = n2;
+                    if (j2 == n2 + 1) j2 = 1;
+                    for (long i = 1; i <= n1 + 1; i++) {
+                        long i1 = i - 1, i2 = i;
+                        if (i1 == 0) i1 = n1;
+                        if (i2 == n1 + 1) i2 = 1;
+                        auto c = [&](long a, long b, long cc, int l) { return u[3 * vidx(a - 1, b - 1, cc - 1) + l]; };
+                        for (int l = 0; l < 3; l++)
+                            un[node(i - 1, j - 1, k - 1) + l] = (c(i2, j2, k2, l) + c(i1, j2, k2, l) + c(i2, j1, k2, l) +
+                                                                 c(i2, j2, k1, l) + c(i1, j1, k2, l) + c(i1, j2, k1, l) +
+                                                                 c(i2, j1, k1, l) + c(i1, j1, k1, l)) * 0.125;
+                    }
+                }
+            }
+            ideriv = 1;
+        } else {
+            for (long k = 0; k < n3node; k++)
+                for (long j = 0; j < nn2; j++)
+                    for (long i = 0; i < nn1; i++) {
+                        auto t = f.read_reals(6);
+                        for (int l = 0; l < 3; l++) un[node(i, j, k) + l] = t[3 + l];
+                    }
+            for (long v = 0; v < N; v++) {
+                long i = v % n1, j = (v / n1) % n2, k = v / ((long)n1 * n2);
+                for (int l = 0; l < 3; l++) u[3 * v + l] = un[node(i, j, k) + l];
+            }
+            ideriv = 2;
+        }
+        // gradient_tensor1: grad(l, m) = d u_l / d x_m = Re ifft(kmod_m * fft(u_l)) / N
+        std::vector<cplx> g3(3 * N), g9(9 * N);
+        for (long v = 0; v < N; v++)
+            for (int l = 0; l < 3; l++) g3[(long)l * N + v] = cplx(u[3 * v + l], 0.0);
+        for (int c = 0; c < 3; c++) fft3_field(&g3[(long)c * N], n1, n2, n3, pf[0], pf[1], pf[2]);
+        for (long v = 0; v < N; v++) {
+            int i = (int)(v % n1) + 1, j = (int)((v / n1) % n2) + 1, k = (int)(v / ((long)n1 * n2)) + 1;
+            double xk[3];
+            spatial_freq(i, j, k, xk);
+            cplx km[3];
+            if (ideriv == 2) {
+                cplx base = cplx(0.0, 1.0) * 0.25 * (1.0 + std::exp(cplx(0.0, xk[0]))) * (1.0 + std::exp(cplx(0.0, xk[1]))) *
+                            (1.0 + std::exp(cplx(0.0, xk[2])));
+                for (int l = 0; l < 3; l++) km[l] = std::tan(xk[l] / 2.0) * base;
+            } else {
+                for (int l = 0; l < 3; l++) km[l] = cplx(0.0, std::sin(xk[l]));
+            }
+            for (int l = 0; l < 3; l++)
+                for (int m = 0; m < 3; m++) g9[(long)(m * 3 + l) * N + v] = g3[(long)l * N + v] * km[m];
+            if ((n1 % 2 == 0 && i == n1 / 2 + 1) && (n2 % 2 == 0 && j == n2 / 2 + 1) && ((n3 % 2 == 0 && k == n3 / 2 + 1) && n3 > 1) &&
+                ideriv == 2)
+                for (int c = 0; c < 9; c++) g9[(long)c * N + v] = 0.0;
+        }
+        for (int c = 0; c < 9; c++) fft3_field(&g9[(long)c * N], n1, n2, n3, pb[0], pb[1], pb[2]);
+        for (long k = 0; k < n3node; k++)
+            for (long j = 0; j < nn2; j++)
+                for (long i = 0; i < nn1; i++) {
+                    long p = 3L * (i + (long)(n1 + 1) * (j + (long)(n2 + 1) * k));
+                    for (int l = 0; l < 3; l++) xnode[p + l] = xnode[p + l] + un[node(i, j, k) + l];
+                }
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) defgradavg[a][b] = (a == b) ? 4.0 : 0.0;  // diag(delt)
+        M3 sc = {}, scs = {}, scg = {};
+        double wsol = 0.0, wgas = 0.0, detFavg = 0.0;
+        bool failed = false;
+        for (long v = 0; v < N; v++) {
+            Voxel& x = vox[v];
+            for (int l = 0; l < 3; l++)
+                for (int m = 0; m < 3; m++) x.F[l][m] = g9[(long)(m * 3 + l) * N + v].real() / (double)N + defgradavg[l][m];
+            copy3(x.F, x.Fini);
+            x.detF = det33(x.F);
+            if (inv3(x.F, x.Finv) != 0) failed = true;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) {
+                    const double t = x.Finv[a][b] * wgt * x.detF;
+                    sc[a][b] = sc[a][b] + t;
+                    if (!x.gas) scs[a][b] = scs[a][b] + t;
+                    if (x.gas) scg[a][b] = scg[a][b] + t;
+                }
+            if (!x.gas) wsol = wsol + wgt * x.detF;
+            if (x.gas) wgas = wgas + wgt * x.detF;
+            x.wgtc = wgt * x.detF;
+            detFavg = detFavg + x.detF * wgt;
+        }
+        if (failed) throw SolveError("Singular matrix in lu_inverse (init_defgrad)", -3);
+        wphcsol = wsol / detFavg;
+        wphcgas = wgas / detFavg;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                defgradinvavgc[a][b] = sc[a][b] / detFavg;
+                defgradinvavgcs[a][b] = scs[a][b] / detFavg / wphcsol;
+                defgradinvavgcg[a][b] = (wphcgas > 0.0) ? scg[a][b] / detFavg / wphcgas : (a == b ? 1.0 : 0.0);
+            }
+        for (long v = 0; v < N; v++) vox[v].wgtc = vox[v].wgtc / detFavg;
     }
 
     // ------------------------------------------------------------ initial_guess (various_functions.f90:8-53)

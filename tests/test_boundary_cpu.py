@@ -53,7 +53,11 @@ def test_valid_deck_reaches_device_check(tmp_path):
     (lambda s: s.replace("\t1       1       0                     |            \n",
                          "\t1       1       1                     |            \n", 1), -1, "boundary"),
     (lambda s: s.replace("2.0 0            XC0", "2.0 3            XC0", 1), -1, "igamma"),
-    (lambda s: s.replace("0                      IDISPINI", "1                      IDISPINI", 1), -2, "IDISPINI"),
+    (lambda s: s.replace("0                      IDISPINI (if idispini=1, next line is filedispl)\n",
+                         "3                      IDISPINI (if idispini=1, next line is filedispl)\nd.txt\n", 1), -1, "idispini"),
+    (lambda s: s.replace("0                      IDISPINI (if idispini=1, next line is filedispl)\n",
+                         "1                      IDISPINI (if idispini=1, next line is filedispl)\n/nonexistent/d.txt\n", 1),
+     -1, "cannot open"),
 ])
 def test_invalid_decks_are_refused(tmp_path, mutate, code, needle):
     fft = decks.write_case(decks.case_c1(nsteps=2), tmp_path)
@@ -70,6 +74,18 @@ def test_discrete_green_decks_are_accepted(tmp_path, igamma):
     fft = decks.write_case(decks.case_c1(nsteps=2), tmp_path)
     fft.write_text(fft.read_text().replace("2.0 0            XC0", f"2.0 {igamma}            XC0", 1))
     rc, msg = _open(fft)
+    assert rc == -6 and "CUDA" in msg
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device path")
+@pytest.mark.parametrize("kind", [1, 2])
+def test_initial_displacement_decks_are_accepted(tmp_path, kind):
+    """IDISPINI 1 (cell centres) and 2 (nodes): the displacement file is read with the deck."""
+    c = decks.case_c1(nsteps=2)
+    c.n = 8
+    c.ngrains = 6
+    c.dispini = kind
+    rc, msg = _open(decks.write_case(c, tmp_path))
     assert rc == -6 and "CUDA" in msg
 
 
