@@ -323,7 +323,7 @@ __device__ __forceinline__ void congruence6(const double* T, const double* A, do
 }
 
 // ---------------------------------------------------------------- k_prologue
-__global__ void __launch_bounds__(kBlock) k_prologue(Dev d, const double* __restrict__ c0g, const double* __restrict__ g0g,
+__global__ void __launch_bounds__(kBlock, 2) k_prologue(Dev d, const double* __restrict__ c0g, const double* __restrict__ g0g,
                                                        int do_schmid, int modal) {
     __shared__ double c0[81], g0[81], c0b[36];
     for (int i = threadIdx.x; i < 81; i += blockDim.x) {
@@ -1213,8 +1213,9 @@ constexpr int kMaxPhaseSmem = 4;
 // Dynamic shared memory of k_newton6p: the staged phases, then per warp the
 // exchange rows, the lanes' columns (Schmid vectors 5 * SPL, resistances
 // crss 2 * SPL, accumulated shear 1; rows of kXStride doubles) and the five
-// groups' sums (70).
-__host__ __device__ constexpr int newton6p_col_rows(int spl) { return 7 * spl + 1; }
+// groups' sums (70).  The lanes' rows of C~ and H0 (12 per lane) and their trial
+// resistances (2 * SPL) are columns too.
+__host__ __device__ constexpr int newton6p_col_rows(int spl) { return 9 * spl + 1 + 12; }
 __host__ __device__ constexpr int newton6p_warp_doubles(int spl) {
     return kXRows * kXStride + newton6p_col_rows(spl) * kXStride + 70;
 }
@@ -1275,15 +1276,15 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     double* const schm = wsm + kXRows * kXStride + lane;
     double* const crsm = schm + 5 * SPL * kXStride;
     double* const gam0 = schm + 7 * SPL * kXStride;
+    double* const crow = gam0 + kXStride;  // row r of C~ (6), then row r of H0 (6)
+    double* const hrow = crow + 6 * kXStride;
+    double* const ttm = hrow + 6 * kXStride;  // trial resistances of the lane's systems (2 per system)
     double* const accw = wsm + kXRows * kXStride + newton6p_col_rows(SPL) * kXStride;
     for (int c = lane; c < 70; c += 32) accw[c] = 0.0;
     __syncwarp();
     double* const accg = accw + (grp < 5 ? grp : 0) * 14;
     const double tolt = fmax(p.error, p.erroral);
     // position of dd(r, j) in the packed upper triangle, for this lane's row
-    int ddq[5];
-#pragma unroll
-    for (int j = 0; j < 5; j++) ddq[j] = (r < j) ? j * (j + 1) / 2 + r : r * (r + 1) / 2 + j;
     const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long v0 = wid * 5; v0 < N; v0 += nwarp * 5) {  // warp-uniform
@@ -1292,7 +1293,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
         const bool gasv = d.gas[v];
         const int phi = d.phase[v];
         // rows r of C~ and H0, q'_r and this lane's systems; no load waits on the gas flag or phase
-        double lam_r, Crow[6], Hrow[6], qp_r, tt[SPL][2];
+        double lam_r, qp_r;
         {
             double lamf[6], sgtf[6], a[9], b6[6], vs[9];
             ld6(d.sg, N, v, a);
@@ -1311,10 +1312,10 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             double cl = 0.0, ss = 0.0;
 #pragma unroll
             for (int j = 0; j < 6; j++) {
-                Crow[j] = d.c066mod[(6 * r + j) * N + v];
+                crow[j * kXStride] = d.c066mod[(6 * r + j) * N + v];
                 const double ci = d.c066inv[(6 * r + j) * N + v];
                 const double sd = d.sg66[(6 * r + j) * N + v] / p.tdot;
-                Hrow[j] = ci + sd;
+                hrow[j * kXStride] = ci + sd;
                 cl += ci * lamf[j];
                 ss += sd * sgtf[j];
             }
@@ -1326,8 +1327,8 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                 const bool any = s < d.nsys;
 #pragma unroll
                 for (int c = 0; c < 5; c++) schm[(5 * k + c) * kXStride] = any ? d.sch[(s * 5 + c) * N + v] : 0.0;
-                tt[k][0] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
-                tt[k][1] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
+                ttm[(2 * k) * kXStride] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
+                ttm[(2 * k + 1) * kXStride] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
                 crsm[(2 * k) * kXStride] = any ? d.crss[(2 * s) * N + v] : 0.0;
                 crsm[(2 * k + 1) * kXStride] = any ? d.crss[(2 * s + 1) * N + v] : 0.0;
             }
@@ -1337,7 +1338,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
         const int nsyst = ph.nsyst;
         const bool gas = valid && gasv;
         const bool act = valid && !gas;
-        double gd[SPL], rs1[SPL], g0s[SPL], nrs[SPL];
+        double gd[SPL], rs1[SPL];
         double taun = 0.0;
 #pragma unroll
         for (int k = 0; k < SPL; k++) {
@@ -1346,11 +1347,10 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             if (!own)
 #pragma unroll
                 for (int c = 0; c < 5; c++) schm[(5 * k + c) * kXStride] = 0.0;
-            g0s[k] = own ? ph.gamd0[s] : 0.0;
-            nrs[k] = own ? ph.nrs[s] : 1.0;
             gd[k] = 0.0;
             rs1[k] = 0.0;
-            taun += tt[k][0] * tt[k][0] + tt[k][1] * tt[k][1];
+            const double t0 = ttm[(2 * k) * kXStride], t1 = ttm[(2 * k + 1) * kXStride];
+            taun += t0 * t0 + t1 * t1;
         }
         const int int_exp = ph.int_exp;
         taun = sqrt(xsum(X, taun));
@@ -1364,18 +1364,23 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             aT = aT && itertau < 10 && errtau > tolt;
             if (!__any_sync(kFull, aT)) break;
             itertau += aT;
+            // residual norms and the Newton correction are compared as squares (no square roots
+            // on the iteration's critical path): resn2 = |res|^2, and the loop runs while
+            // |dsg|^2 > (erroral |sg_in|)^2
             int iterNR = 0;
-            double erral = 2.0 * p.erroral, resoldn = 1.0;
+            double resoldn2 = 1.0;
+            bool more = true;
+            const double errlim2 = (p.erroral * sgnorm) * (p.erroral * sgnorm);
             bool aN = aT;
             while (true) {
-                aN = aN && iterNR < 100 && erral > p.erroral;
+                aN = aN && iterNR < 100 && more;
                 if (!__any_sync(kFull, aN)) break;
                 iterNR += aN;
                 int icut = 0;
-                double resn = 2.0 * resoldn, rho_c = 0.0;
+                double resn2 = 4.0 * resoldn2, rho_c = 0.0;
                 bool aC = aN;
                 while (true) {
-                    aC = aC && resn > resoldn && icut < 10;
+                    aC = aC && resn2 > resoldn2 && icut < 10;
                     if (!__any_sync(kFull, aC)) break;
                     // plastic_strain_rate at sg (own systems)
                     double sgf[6];
@@ -1390,10 +1395,11 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
 #pragma unroll
                             for (int c = 0; c < 5; c++) sc[c] = schm[(5 * k + c) * kXStride];
                             double rss = sc[0] * sgf[0] + sc[1] * sgf[1] + sc[2] * sgf[2] + sc[3] * sgf[3] + sc[4] * sgf[4];
-                            const double tau = (rss - 0.0 < 0.0) ? tt[k][1] : tt[k][0];
+                            const double tau = ttm[(2 * k + ((rss - 0.0 < 0.0) ? 1 : 0)) * kXStride];
                             rss = (rss - 0.0) / tau;
-                            const double dum = g0s[k] * powabs(rss, nrs[k] - 1.0, int_exp);
-                            rsn[k] = nrs[k] * dum / tau;
+                            const double nk = ph.nrs[r + 6 * k];
+                            const double dum = ph.gamd0[r + 6 * k] * powabs(rss, nk - 1.0, int_exp);
+                            rsn[k] = nk * dum / tau;
                             gdn[k] = rss * dum;
 #pragma unroll
                             for (int c = 0; c < 5; c++) ep[c] += sc[c] * gdn[k];
@@ -1411,13 +1417,13 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                     }
                     double rho = epr - qp_r;
 #pragma unroll
-                    for (int j = 0; j < 6; j++) rho += Hrow[j] * sgf[j];
+                    for (int j = 0; j < 6; j++) rho += hrow[j * kXStride] * sgf[j];
                     double rhof[6];
                     xgather(X, rho, rhof);
                     double rn = 0.0;
 #pragma unroll
-                    for (int j = 0; j < 6; j++) rn += Crow[j] * rhof[j];
-                    const double rnn = sqrt(xsum(X, rn * rn));
+                    for (int j = 0; j < 6; j++) rn += crow[j * kXStride] * rhof[j];
+                    const double rnn2 = xsum(X, rn * rn);
                     if (aC) {
 #pragma unroll
                         for (int k = 0; k < SPL; k++) {
@@ -1427,14 +1433,14 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                         edotp_r = epr;
                         sev_r = sg_r;
                         rho_c = rho;
-                        resn = rnn;
-                        if (iterNR == 1) resoldn = resn;
-                        if (resn > resoldn) sg_r = sgold_r + (sg_r - sgold_r) * 0.5;
+                        resn2 = rnn2;
+                        if (iterNR == 1) resoldn2 = resn2;
+                        if (resn2 > resoldn2) sg_r = sgold_r + (sg_r - sgold_r) * 0.5;
                         icut++;
                     }
                 }
                 if (aN) {
-                    resoldn = resn;
+                    resoldn2 = resn2;
                     sgold_r = sg_r;
                 }
                 // d(edotp)/d(sigma), packed upper triangle, partial over this lane's systems
@@ -1465,10 +1471,11 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                 for (int j = 0; j < 6; j++) {
                     double x = 0.0;
                     if (j < 5 && r < 5) {
-                        const double* e = X.P + ddq[j] * kXStride + base;
+                        const int q = (r < j) ? j * (j + 1) / 2 + r : r * (r + 1) / 2 + j;  // dd(r, j), packed
+                        const double* e = X.P + q * kXStride + base;
                         x = ((((e[0] + e[1]) + e[2]) + e[3]) + e[4]) + e[5];
                     }
-                    Hr[j] = Hrow[j] + x;
+                    Hr[j] = hrow[j * kXStride] + x;
                 }
                 // Gauss-Jordan elimination in the fixed order 0..5 (H is positive definite)
                 double b = rho_c;
@@ -1492,7 +1499,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                 if (aN) {
                     if (sing && r == 0) set_err(d.err, 1);
                     sg_r = sg_new;
-                    erral = sqrt(dsgnr) / sgnorm;
+                    more = sgnorm > 0.0 ? dsgnr > errlim2 : dsgnr > 0.0;
                 }
             }
             if (p.iuphard) {  // harden (various_functions.f90:1439-1491)
@@ -1539,14 +1546,15 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                         tn[k][0] = crsm[(2 * k) * kXStride] + dtau * voce * p.tdot / deltgam;
                         tn[k][1] = crsm[(2 * k + 1) * kXStride] + dtau * voce * p.tdot / deltgam;
                     }
-                    e2 += (tt[k][0] - tn[k][0]) * (tt[k][0] - tn[k][0]) + (tt[k][1] - tn[k][1]) * (tt[k][1] - tn[k][1]);
+                    const double d0 = ttm[(2 * k) * kXStride] - tn[k][0], d1 = ttm[(2 * k + 1) * kXStride] - tn[k][1];
+                    e2 += d0 * d0 + d1 * d1;
                 }
                 const double et = sqrt(xsum(X, e2)) / taun;
                 if (aT) {
 #pragma unroll
                     for (int k = 0; k < SPL; k++) {
-                        tt[k][0] = tn[k][0];
-                        tt[k][1] = tn[k][1];
+                        ttm[(2 * k) * kXStride] = tn[k][0];
+                        ttm[(2 * k + 1) * kXStride] = tn[k][1];
                     }
                     errtau = et;
                 }
@@ -1597,8 +1605,8 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                 const int s = r + 6 * k;
                 if (s < d.nsys) {
                     d.gamdot[s * N + v] = (s < nsyst) ? gd[k] : 0.0;
-                    d.trialtau[(2 * s) * N + v] = tt[k][0];
-                    d.trialtau[(2 * s + 1) * N + v] = tt[k][1];
+                    d.trialtau[(2 * s) * N + v] = ttm[(2 * k) * kXStride];
+                    d.trialtau[(2 * s + 1) * N + v] = ttm[(2 * k + 1) * kXStride];
                 }
             }
             if (r == 0) {
@@ -1906,7 +1914,7 @@ void launch_upd2(const Dev& d, const Upd2Params& p, cudaStream_t st) { k_upd2<<<
 
 // ---------------------------------------------------------------- k_upd3
 template <int NS>
-__global__ void __launch_bounds__(kBlock) k_upd3(Dev d, Upd3Params p) {
+__global__ void __launch_bounds__(kBlock, 2) k_upd3(Dev d, Upd3Params p) {
     const long long N = d.N;
     __shared__ double du[9];
     if (threadIdx.x < 9) du[threadIdx.x] = p.iupdate ? __ldcg(&d.red[OFF_DU2 + threadIdx.x]) : 0.0;
@@ -1995,7 +2003,7 @@ __device__ __forceinline__ MinIdx min_last(MinIdx a, MinIdx b) {
     if (a.v < b.v) return a;
     return (b.i > a.i) ? b : a;
 }
-__global__ void __launch_bounds__(kBlock) k_diag(Dev d, double Lfloor) {
+__global__ void __launch_bounds__(kBlock, 2) k_diag(Dev d, double Lfloor) {
     const long long N = d.N;
     double s[6] = {0, 0, 0, 0, 0, 0};
     double m[13];
