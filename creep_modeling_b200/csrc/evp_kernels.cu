@@ -1201,26 +1201,48 @@ __device__ __forceinline__ void xgather(const Xw& X, double x, double (&out)[6])
     for (int c = 0; c < 6; c++) out[c] = row[X.base + c];
 }
 
-// What the local solve reads of a phase, staged in shared memory once per block.
+// What the local solve reads of a phase, staged in shared memory once per block
+// (MS systems at most: 12 or 24).
+template <int MS>
 struct PhaseN {
     int nsyst, nmodes, int_exp, nsm[3];
-    double nrs[kMaxSysDev], gamd0[kMaxSysDev];
+    double nrs[MS], gamd0[MS];
     double tau1[3], thet0[3], thet1[3];
-    double hard[kMaxSysDev * kMaxSysDev];
+    double hard[MS * MS];
 };
 constexpr int kMaxPhaseSmem = 4;
 
+// N doubles owned by a lane: a column of the warp's shared memory (entries kXStride
+// apart) when SM, else registers (every index must then be a compile-time constant).
+template <bool SM, int N>
+struct LaneCol {
+    double* p;
+    double r[SM ? 1 : N];
+    __device__ __forceinline__ double& operator[](int i) {
+        if constexpr (SM) return p[i * kXStride];
+        else return r[i];
+    }
+};
+
 // Dynamic shared memory of k_newton6p: the staged phases, then per warp the
-// exchange rows, the lanes' columns (Schmid vectors 5 * SPL, resistances
-// crss 2 * SPL, accumulated shear 1; rows of kXStride doubles) and the five
-// groups' sums (70).  The lanes' rows of C~ and H0 (12 per lane) and their trial
-// resistances (2 * SPL) are columns too.
-__host__ __device__ constexpr int newton6p_col_rows(int spl) { return 9 * spl + 1 + 12; }
+// exchange rows, the lanes' columns (rows of kXStride doubles) and the five
+// groups' sums (70).  The columns hold the Schmid vectors (5 * SPL) and, with
+// two systems per lane (12-system phases), also the lane's rows of C~ and H0
+// (12), its trial resistances (2 * SPL), accepted slip rates and rate factors
+// (2 * SPL) and three stress/strain-rate components: kept out of registers,
+// they leave the Newton loop nearly free of spills, and two blocks of 256
+// threads still fit one SM.  With four systems per lane those stay in registers
+// (the larger columns would leave room for one block per SM).
+__host__ __device__ constexpr bool newton6p_cols_in_smem(int spl) { return spl == 2; }
+__host__ __device__ constexpr int newton6p_col_rows(int spl) {
+    return 5 * spl + (newton6p_cols_in_smem(spl) ? 12 + 4 * spl + 3 : 0);
+}
 __host__ __device__ constexpr int newton6p_warp_doubles(int spl) {
     return kXRows * kXStride + newton6p_col_rows(spl) * kXStride + 70;
 }
 __host__ __device__ constexpr size_t newton6p_smem_bytes(int spl, int nph) {
-    return (size_t)nph * sizeof(PhaseN) + 8 * sizeof(double) * (size_t)newton6p_warp_doubles(spl);
+    return (size_t)nph * (spl == 2 ? sizeof(PhaseN<12>) : sizeof(PhaseN<24>)) +
+           8 * sizeof(double) * (size_t)newton6p_warp_doubles(spl);
 }
 
 // ---------------------------------------------------------------- k_newton6p: symmetric positive definite form
@@ -1242,8 +1264,10 @@ __host__ __device__ constexpr size_t newton6p_smem_bytes(int spl, int nph) {
 // memory, which keeps the kernel within 128 registers (16 warps per SM).
 template <int SPL>
 __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
+    constexpr int MS = 6 * SPL;
+    constexpr bool kSm = newton6p_cols_in_smem(SPL);
     extern __shared__ double dyn_smem[];
-    PhaseN* const sph = reinterpret_cast<PhaseN*>(dyn_smem);
+    PhaseN<MS>* const sph = reinterpret_cast<PhaseN<MS>*>(dyn_smem);
     const int nph = d.nph < kMaxPhaseSmem ? d.nph : kMaxPhaseSmem;
     for (int q = threadIdx.x; q < nph; q += blockDim.x) {
         const PhaseDev& g = d.ph[q];
@@ -1257,13 +1281,14 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             sph[q].thet1[m] = g.thet1[m];
         }
     }
-    for (int e = threadIdx.x; e < nph * kMaxSysDev; e += blockDim.x) {
-        sph[e / kMaxSysDev].nrs[e % kMaxSysDev] = d.ph[e / kMaxSysDev].nrs[e % kMaxSysDev];
-        sph[e / kMaxSysDev].gamd0[e % kMaxSysDev] = d.ph[e / kMaxSysDev].gamd0[e % kMaxSysDev];
+    for (int e = threadIdx.x; e < nph * MS; e += blockDim.x) {
+        sph[e / MS].nrs[e % MS] = d.ph[e / MS].nrs[e % MS];
+        sph[e / MS].gamd0[e % MS] = d.ph[e / MS].gamd0[e % MS];
     }
-    for (int e = threadIdx.x; e < nph * kMaxSysDev * kMaxSysDev; e += blockDim.x)
-        sph[e / (kMaxSysDev * kMaxSysDev)].hard[e % (kMaxSysDev * kMaxSysDev)] =
-            d.ph[e / (kMaxSysDev * kMaxSysDev)].hard[e % (kMaxSysDev * kMaxSysDev)];
+    for (int e = threadIdx.x; e < nph * MS * MS; e += blockDim.x) {
+        const int q = e / (MS * MS), i = (e % (MS * MS)) / MS, j = e % MS;
+        sph[q].hard[i * MS + j] = d.ph[q].hard[i * kMaxSysDev + j];
+    }
     __syncthreads();
     double* const wsm = reinterpret_cast<double*>(sph + nph) + (threadIdx.x >> 5) * newton6p_warp_doubles(SPL);
     const long long N = d.N;
@@ -1272,13 +1297,16 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     const int r = lane - 6 * grp;             // row / component owned by this lane
     const int base = grp < 5 ? 6 * grp : 24;  // idle lanes shadow group 4's lanes and write nothing
     const Xw X{wsm, lane, base};
-    // this lane's column: Schmid vectors, resistances, accumulated shear
+    // this lane's column: Schmid vectors, then (kSm) the values below
     double* const schm = wsm + kXRows * kXStride + lane;
-    double* const crsm = schm + 5 * SPL * kXStride;
-    double* const gam0 = schm + 7 * SPL * kXStride;
-    double* const crow = gam0 + kXStride;  // row r of C~ (6), then row r of H0 (6)
-    double* const hrow = crow + 6 * kXStride;
-    double* const ttm = hrow + 6 * kXStride;  // trial resistances of the lane's systems (2 per system)
+    double* const col = schm + 5 * SPL * kXStride;
+    LaneCol<kSm, 6> Crow{col}, Hrow{col + 6 * kXStride};    // rows r of C~ and H0
+    LaneCol<kSm, 2 * SPL> TT{col + 12 * kXStride};          // trial resistances of the lane's systems
+    LaneCol<kSm, SPL> GD{col + (12 + 2 * SPL) * kXStride};  // accepted slip rates
+    LaneCol<kSm, SPL> RS{col + (12 + 3 * SPL) * kXStride};  // and their d(rate)/d(tau) factors
+    LaneCol<kSm, 1> LAM{col + (12 + 4 * SPL) * kXStride};   // component r of the input stress,
+    LaneCol<kSm, 1> SEV{col + (13 + 4 * SPL) * kXStride};   // of the stress at the last accepted evaluation
+    LaneCol<kSm, 1> EPM{col + (14 + 4 * SPL) * kXStride};   // and of the plastic strain rate there
     double* const accw = wsm + kXRows * kXStride + newton6p_col_rows(SPL) * kXStride;
     for (int c = lane; c < 70; c += 32) accw[c] = 0.0;
     __syncwarp();
@@ -1293,7 +1321,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
         const bool gasv = d.gas[v];
         const int phi = d.phase[v];
         // rows r of C~ and H0, q'_r and this lane's systems; no load waits on the gas flag or phase
-        double lam_r, qp_r;
+        double qp_r;
         {
             double lamf[6], sgtf[6], a[9], b6[6], vs[9];
             ld6(d.sg, N, v, a);
@@ -1312,33 +1340,30 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             double cl = 0.0, ss = 0.0;
 #pragma unroll
             for (int j = 0; j < 6; j++) {
-                crow[j * kXStride] = d.c066mod[(6 * r + j) * N + v];
+                Crow[j] = d.c066mod[(6 * r + j) * N + v];
                 const double ci = d.c066inv[(6 * r + j) * N + v];
                 const double sd = d.sg66[(6 * r + j) * N + v] / p.tdot;
-                hrow[j * kXStride] = ci + sd;
+                Hrow[j] = ci + sd;
                 cl += ci * lamf[j];
                 ss += sd * sgtf[j];
             }
             qp_r = cl + ss + De;
-            lam_r = sel6(lamf, r);
+            LAM[0] = sel6(lamf, r);
 #pragma unroll
             for (int k = 0; k < SPL; k++) {
                 const int s = r + 6 * k;
                 const bool any = s < d.nsys;
 #pragma unroll
                 for (int c = 0; c < 5; c++) schm[(5 * k + c) * kXStride] = any ? d.sch[(s * 5 + c) * N + v] : 0.0;
-                ttm[(2 * k) * kXStride] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
-                ttm[(2 * k + 1) * kXStride] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
-                crsm[(2 * k) * kXStride] = any ? d.crss[(2 * s) * N + v] : 0.0;
-                crsm[(2 * k + 1) * kXStride] = any ? d.crss[(2 * s + 1) * N + v] : 0.0;
+                TT[2 * k] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
+                TT[2 * k + 1] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
             }
-            *gam0 = d.gacumgr[v];
         }
-        const PhaseN& ph = sph[phi];
+        const PhaseN<MS>& ph = sph[phi];
         const int nsyst = ph.nsyst;
         const bool gas = valid && gasv;
         const bool act = valid && !gas;
-        double gd[SPL], rs1[SPL];
+
         double taun = 0.0;
 #pragma unroll
         for (int k = 0; k < SPL; k++) {
@@ -1347,16 +1372,18 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             if (!own)
 #pragma unroll
                 for (int c = 0; c < 5; c++) schm[(5 * k + c) * kXStride] = 0.0;
-            gd[k] = 0.0;
-            rs1[k] = 0.0;
-            const double t0 = ttm[(2 * k) * kXStride], t1 = ttm[(2 * k + 1) * kXStride];
+            GD[k] = 0.0;
+            RS[k] = 0.0;
+            const double t0 = TT[2 * k], t1 = TT[2 * k + 1];
             taun += t0 * t0 + t1 * t1;
         }
         const int int_exp = ph.int_exp;
         taun = sqrt(xsum(X, taun));
-        double sg_r = lam_r;
+        double sg_r = LAM[0];
         const double sgnorm = sqrt(xsum(X, sg_r * sg_r));
-        double sgold_r = 0.0, sev_r = 0.0, edotp_r = 0.0;
+        double sgold_r = 0.0;
+        SEV[0] = 0.0;
+        EPM[0] = 0.0;
         int itertau = 0;
         double errtau = 2.0 * tolt;
         bool aT = act;
@@ -1395,7 +1422,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
 #pragma unroll
                             for (int c = 0; c < 5; c++) sc[c] = schm[(5 * k + c) * kXStride];
                             double rss = sc[0] * sgf[0] + sc[1] * sgf[1] + sc[2] * sgf[2] + sc[3] * sgf[3] + sc[4] * sgf[4];
-                            const double tau = ttm[(2 * k + ((rss - 0.0 < 0.0) ? 1 : 0)) * kXStride];
+                            const double tau = (rss - 0.0 < 0.0) ? TT[2 * k + 1] : TT[2 * k];
                             rss = (rss - 0.0) / tau;
                             const double nk = ph.nrs[r + 6 * k];
                             const double dum = ph.gamd0[r + 6 * k] * powabs(rss, nk - 1.0, int_exp);
@@ -1417,21 +1444,21 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                     }
                     double rho = epr - qp_r;
 #pragma unroll
-                    for (int j = 0; j < 6; j++) rho += hrow[j * kXStride] * sgf[j];
+                    for (int j = 0; j < 6; j++) rho += Hrow[j] * sgf[j];
                     double rhof[6];
                     xgather(X, rho, rhof);
                     double rn = 0.0;
 #pragma unroll
-                    for (int j = 0; j < 6; j++) rn += crow[j * kXStride] * rhof[j];
+                    for (int j = 0; j < 6; j++) rn += Crow[j] * rhof[j];
                     const double rnn2 = xsum(X, rn * rn);
                     if (aC) {
 #pragma unroll
                         for (int k = 0; k < SPL; k++) {
-                            gd[k] = gdn[k];
-                            rs1[k] = rsn[k];
+                            GD[k] = gdn[k];
+                            RS[k] = rsn[k];
                         }
-                        edotp_r = epr;
-                        sev_r = sg_r;
+                        EPM[0] = epr;
+                        SEV[0] = sg_r;
                         rho_c = rho;
                         resn2 = rnn2;
                         if (iterNR == 1) resoldn2 = resn2;
@@ -1459,7 +1486,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                             double x = 0.0;
 #pragma unroll
                             for (int k = 0; k < SPL; k++)
-                                if (r + 6 * k < nsyst) x += sc[k][ii] * sc[k][jj] * rs1[k];
+                                if (r + 6 * k < nsyst) x += sc[k][ii] * sc[k][jj] * RS[k];
                             X.P[q * kXStride + lane] = x;
                             q++;
                         }
@@ -1475,7 +1502,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                         const double* e = X.P + q * kXStride + base;
                         x = ((((e[0] + e[1]) + e[2]) + e[3]) + e[4]) + e[5];
                     }
-                    Hr[j] = hrow[j * kXStride] + x;
+                    Hr[j] = Hrow[j] + x;
                 }
                 // Gauss-Jordan elimination in the fixed order 0..5 (H is positive definite)
                 double b = rho_c;
@@ -1506,18 +1533,15 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                 double dg = 0.0;
 #pragma unroll
                 for (int k = 0; k < SPL; k++)
-                    if (r + 6 * k < nsyst) dg += fabs(gd[k]) * p.tdot;
+                    if (r + 6 * k < nsyst) dg += fabs(GD[k]) * p.tdot;
                 const double deltgam = xsum(X, dg);
-                const double gamma0 = *gam0;
+                const double gamma0 = d.gacumgr[v];
                 const double gamma1 = gamma0 + deltgam;
-                double gall[6 * SPL];
+                // |slip rate| of the group's system 6k + q in exchange row k, column base + q
+                __syncwarp();
 #pragma unroll
-                for (int k = 0; k < SPL; k++) {
-                    double t6[6];
-                    xgather(X, fabs(gd[k]), t6);
-#pragma unroll
-                    for (int q = 0; q < 6; q++) gall[6 * k + q] = t6[q];
-                }
+                for (int k = 0; k < SPL; k++) X.P[k * kXStride + lane] = fabs(GD[k]);
+                __syncwarp();
                 double e2 = 0.0, tn[SPL][2];
                 int vmode = -1;  // mode whose Voce increment is in voce (systems of one mode share it)
                 double voce = 0.0;
@@ -1542,19 +1566,19 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                         double dtau = 0.0;
 #pragma unroll
                         for (int js = 0; js < 6 * SPL; js++)
-                            if (js < nsyst) dtau = dtau + ph.hard[s * kMaxSysDev + js] * gall[js];
-                        tn[k][0] = crsm[(2 * k) * kXStride] + dtau * voce * p.tdot / deltgam;
-                        tn[k][1] = crsm[(2 * k + 1) * kXStride] + dtau * voce * p.tdot / deltgam;
+                            if (js < nsyst) dtau = dtau + ph.hard[s * MS + js] * X.P[(js / 6) * kXStride + base + js % 6];
+                        tn[k][0] = d.crss[(2 * s) * N + v] + dtau * voce * p.tdot / deltgam;
+                        tn[k][1] = d.crss[(2 * s + 1) * N + v] + dtau * voce * p.tdot / deltgam;
                     }
-                    const double d0 = ttm[(2 * k) * kXStride] - tn[k][0], d1 = ttm[(2 * k + 1) * kXStride] - tn[k][1];
+                    const double d0 = TT[2 * k] - tn[k][0], d1 = TT[2 * k + 1] - tn[k][1];
                     e2 += d0 * d0 + d1 * d1;
                 }
                 const double et = sqrt(xsum(X, e2)) / taun;
                 if (aT) {
 #pragma unroll
                     for (int k = 0; k < SPL; k++) {
-                        ttm[(2 * k) * kXStride] = tn[k][0];
-                        ttm[(2 * k + 1) * kXStride] = tn[k][1];
+                        TT[2 * k] = tn[k][0];
+                        TT[2 * k + 1] = tn[k][1];
                     }
                     errtau = et;
                 }
@@ -1582,17 +1606,17 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
         }
         {
             double dsf[6];
-            xgather(X, (sev_r - sgt_r) / p.tdot, dsf);
+            xgather(X, (SEV[0] - sgt_r) / p.tdot, dsf);
 #pragma unroll
             for (int j = 0; j < 6; j++) ee += d.sg66[(6 * r + j) * N + v] * dsf[j];
         }
-        double edot_r = edotp_r + ee;
+        double edot_r = EPM[0] + ee;
         if (p.thermo) edot_r = edot_r + eth_r;
-        const double dl = sg_r - lam_r, de = edot_r - D_r;
+        const double dl = sg_r - LAM[0], de = edot_r - D_r;
         const double dsgnorm = xsum(X, dl * dl), ddgnorm = xsum(X, de * de);
         // outputs: sigma and edotp in the symmetric 3x3 form, slip rates and resistances
         xgather(X, sg_r, sgf);
-        xgather(X, edotp_r, epf);
+        xgather(X, EPM[0], epf);
         epf[5] = 0.0;
         if (act) {
             double s6v[6], e6v[6];
@@ -1604,9 +1628,9 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             for (int k = 0; k < SPL; k++) {
                 const int s = r + 6 * k;
                 if (s < d.nsys) {
-                    d.gamdot[s * N + v] = (s < nsyst) ? gd[k] : 0.0;
-                    d.trialtau[(2 * s) * N + v] = ttm[(2 * k) * kXStride];
-                    d.trialtau[(2 * s + 1) * N + v] = ttm[(2 * k + 1) * kXStride];
+                    d.gamdot[s * N + v] = (s < nsyst) ? GD[k] : 0.0;
+                    d.trialtau[(2 * s) * N + v] = TT[2 * k];
+                    d.trialtau[(2 * s + 1) * N + v] = TT[2 * k + 1];
                 }
             }
             if (r == 0) {
