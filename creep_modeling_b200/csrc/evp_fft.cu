@@ -136,31 +136,44 @@ __device__ __forceinline__ void fft_stage(CT* s, int ES, int P, int n, int Ns, c
     __syncthreads();
 }
 
-// Radix sets: RS = 0 compiles the power-of-two radices only (2, 4, 8; two
-// butterflies per thread), RS = 1 every radix (four butterflies per thread).
-// The power-of-two kernels fit 128 registers, so two blocks of 256 threads
-// are resident per SM where the all-radix kernels (255 registers) allow one.
-template <int RS>
-__host__ __device__ constexpr int fft_maxb() { return RS == 0 ? 2 : 4; }
+// Radix sets: RS = 0 compiles the power-of-two radices only (2, 4, 8), RS = 1
+// every radix.  Butterflies per thread fall with the radix so that no stage
+// holds more than 16 complex values per thread: two for every power-of-two
+// radix with RS = 0; four for radices 2-4, two for 5-8 and one for 11 and 13
+// with RS = 1.  Every kernel then fits 128 registers, two blocks of 256
+// threads per SM; the launchers size blocks for the stage that needs the most
+// threads (stage_threads).
+__host__ __device__ constexpr int fft_maxb_r(int rs, int R) { return rs == 0 ? 2 : (R <= 4 ? 4 : (R <= 8 ? 2 : 1)); }
 
-template <bool INV, int RS, class CT>
+// An odd-radix stage as a function of its own (ODD_CALL in fft_run): its registers are
+// then allocated apart from a kernel with a heavy epilogue (the grid-update z pass).
+template <int R, bool INV, int MAXB, class CT>
+__device__ __noinline__ void fft_stage_call(CT* s, int ES, int P, int n, int Ns, const CT* __restrict__ tw) {
+    fft_stage<R, INV, MAXB, CT>(s, ES, P, n, Ns, tw);
+}
+template <int R, bool INV, int MAXB, class CT, bool CALL>
+__device__ __forceinline__ void fft_stage_odd(CT* s, int ES, int P, int n, int Ns, const CT* __restrict__ tw) {
+    if constexpr (CALL) fft_stage_call<R, INV, MAXB, CT>(s, ES, P, n, Ns, tw);
+    else fft_stage<R, INV, MAXB, CT>(s, ES, P, n, Ns, tw);
+}
+
+template <bool INV, int RS, class CT, bool ODD_CALL = false>
 __device__ void fft_run(CT* s, int ES, int P, const FftPlan1D& pl, const CT* __restrict__ tw) {
-    constexpr int MB = fft_maxb<RS>();
     int Ns = 1;
     for (int st = 0; st < pl.nst; st++) {
         const int R = pl.rad[st];
         switch (R) {
-            case 2: fft_stage<2, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
-            case 4: fft_stage<4, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
-            case 8: fft_stage<8, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+            case 2: fft_stage<2, INV, fft_maxb_r(RS, 2), CT>(s, ES, P, pl.n, Ns, tw); break;
+            case 4: fft_stage<4, INV, fft_maxb_r(RS, 4), CT>(s, ES, P, pl.n, Ns, tw); break;
+            case 8: fft_stage<8, INV, fft_maxb_r(RS, 8), CT>(s, ES, P, pl.n, Ns, tw); break;
             default:
                 if constexpr (RS != 0) {
                     switch (R) {
-                        case 3: fft_stage<3, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
-                        case 5: fft_stage<5, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
-                        case 7: fft_stage<7, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
-                        case 11: fft_stage<11, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
-                        case 13: fft_stage<13, INV, MB, CT>(s, ES, P, pl.n, Ns, tw); break;
+                        case 3: fft_stage_odd<3, INV, fft_maxb_r(RS, 3), CT, ODD_CALL>(s, ES, P, pl.n, Ns, tw); break;
+                        case 5: fft_stage_odd<5, INV, fft_maxb_r(RS, 5), CT, ODD_CALL>(s, ES, P, pl.n, Ns, tw); break;
+                        case 7: fft_stage_odd<7, INV, fft_maxb_r(RS, 7), CT, ODD_CALL>(s, ES, P, pl.n, Ns, tw); break;
+                        case 11: fft_stage_odd<11, INV, fft_maxb_r(RS, 11), CT, ODD_CALL>(s, ES, P, pl.n, Ns, tw); break;
+                        case 13: fft_stage_odd<13, INV, fft_maxb_r(RS, 13), CT, ODD_CALL>(s, ES, P, pl.n, Ns, tw); break;
                         default: break;
                     }
                 }
@@ -196,10 +209,15 @@ FftPlan1D make_plan(int n) {
     if (m != 1) throw std::runtime_error("unsupported FFT length " + std::to_string(n) + " (prime factors must be <= 13)");
     return pl;
 }
-static int min_radix(const FftPlan1D& pl) {
-    int r = 64;
-    for (int i = 0; i < pl.nst; i++) r = pl.rad[i] < r ? pl.rad[i] : r;
-    return pl.nst ? r : 1;
+// threads that cover every stage of the plan for `pencils` pencils (radix set rs)
+static long long stage_threads(const FftPlan1D& pl, long long pencils, int rs) {
+    long long t = 1;
+    for (int i = 0; i < pl.nst; i++) {
+        const int R = pl.rad[i], mb = fft_maxb_r(rs, R);
+        const long long b = (pencils * (pl.n / R) + mb - 1) / mb;
+        t = b > t ? b : t;
+    }
+    return t;
 }
 
 // twiddle table of an axis in the complex type of the pass
@@ -217,7 +235,7 @@ __device__ __forceinline__ const float2* twid<float2>(const Dev& d, int axis) {
 // ---------------------------------------------------------------- x forward (R2C)
 // mode 0: P'_ij = J * ((sigma - <sigma>) F^{-T})_ij ; mode 1: (L F)_ij (grid update)
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
+__global__ void __launch_bounds__(256, 2) k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
     using Re = typename CxT<CT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
@@ -280,7 +298,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_fwd(Dev d, FftPl
 
 // ---------------------------------------------------------------- y (C2C)
 template <bool INV, int RS, class CT>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_y(Dev d, FftPlan1D pl, int T) {
+__global__ void __launch_bounds__(256, 2) k_fft_y(Dev d, FftPlan1D pl, int T) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
     const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
@@ -325,7 +343,7 @@ __device__ __forceinline__ int inv3_any(const float* a, float* ai) {
 }
 
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
+__global__ void __launch_bounds__(256, 2) k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
     using Re = typename CxT<CT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
@@ -430,7 +448,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_green(Dev d, Fft
 
 // ---------------------------------------------------------------- z fused with the spectral integration (grid update)
 template <int RS>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
+__global__ void __launch_bounds__(256, 2) k_fft_z_integ(Dev d, FftPlan1D pl, int T, int ideriv) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
     const int kx0 = blockIdx.x * T, j = blockIdx.y;
@@ -441,7 +459,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
         s[k3 * P + c * T + t] = (kx < n1h) ? d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    fft_run<false, RS, double2>(s, P, P, pl, d.tw3);
+    fft_run<false, RS, double2, true>(s, P, P, pl, d.tw3);
     if (blockIdx.x == 0 && j == 0 && threadIdx.x < 9) {
         const double2 z = s[threadIdx.x * T];
         d.red[OFF_DC + 2 * threadIdx.x] = z.x;
@@ -486,7 +504,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
         for (int l = 0; l < 3; l++) q[l * T] = u[l];
     }
     __syncthreads();
-    fft_run<true, RS, double2>(s, P, 3 * T, pl, d.tw3);
+    fft_run<true, RS, double2, true>(s, P, 3 * T, pl, d.tw3);
     for (int idx = threadIdx.x; idx < 3 * T * n3; idx += blockDim.x) {
         const int t = idx % T, r = idx / T, c = r % 3, k3 = r / 3, kx = kx0 + t;
         if (kx < n1h) d.spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
@@ -499,7 +517,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_integ(Dev d, Fft
 // point where all three Nyquist planes meet), so the inverse gives d u_l / d x_m
 // (gradient_tensor1, various_functions.f90:56-112).
 template <int RS>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_grad(Dev d, FftPlan1D pl, int T, int ideriv) {
+__global__ void __launch_bounds__(256, 2) k_fft_z_grad(Dev d, FftPlan1D pl, int T, int ideriv) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
     const int kx0 = blockIdx.x * T, j = blockIdx.y;
@@ -549,7 +567,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_z_grad(Dev d, FftP
 
 // ---------------------------------------------------------------- x inverse (C2R)
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
+__global__ void __launch_bounds__(256, 2) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
     using Re = typename CxT<CT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
@@ -652,7 +670,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_fft_x_inv(Dev d, FftPl
 // x passes of evp_green_apply: the 9 real input fields come straight from a
 // caller-owned array tau[c*N + v] and the result goes to out[c*N + v].
 template <int RS>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restrict__ tau) {
+__global__ void __launch_bounds__(256, 2) k_green_x_fwd(Dev d, FftPlan1D pl, int G, const double* __restrict__ tau) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
@@ -681,7 +699,7 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_fwd(Dev d, Fft
     }
 }
 template <int RS>
-__global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ out) {
+__global__ void __launch_bounds__(256, 2) k_green_x_inv(Dev d, FftPlan1D pl, int G, double* __restrict__ out) {
     extern __shared__ double2 s[];
     const int n1 = d.n1, n1h = d.n1h;
     const long long N = d.N;
@@ -715,8 +733,8 @@ __global__ void __launch_bounds__(256, RS == 0 ? 2 : 1) k_green_x_inv(Dev d, Fft
 }
 
 // ---------------------------------------------------------------- launchers
-// A pass needs P * n / (smallest radix) / (butterflies per thread) threads for
-// P pencils of length n.  Each launcher picks the power-of-two kernels when the
+// A pass needs, for P pencils of length n, the largest over its stages of
+// P * (n / R) / (butterflies per thread at radix R) threads.  Each launcher picks the power-of-two kernels when the
 // plan has only radices 2, 4 and 8, asks the kernel for its block-size limit
 // (set by its register use) and shrinks its tile (pencils per block) until
 // the threads fit.
@@ -731,10 +749,10 @@ static int kernel_max_threads(const void* k) {
     return a.maxThreadsPerBlock;
 }
 // largest tile T <= T0 whose ncomp * T pencils fit in maxthr threads; thr gets the block size
-static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int maxb, int want, int maxthr, int& thr) {
+static int fit_tile(int T0, int ncomp, const FftPlan1D& pl, int rs, int want, int maxthr, int& thr) {
     for (int T = T0; T >= 1; T--) {
-        const int need = (ncomp * T * pl.n / min_radix(pl) + maxb - 1) / maxb;
-        int t = want > need ? want : need;
+        const long long need = stage_threads(pl, (long long)ncomp * T, rs);
+        int t = want > need ? want : (int)need;
         t = (t + 31) / 32 * 32;
         if (t > maxthr) t = maxthr / 32 * 32;
         if (need <= t) {
@@ -759,13 +777,13 @@ static int sm_count() {
 // least (waves of blocks) x (T + 1): block time grows with T, and a last wave
 // that is mostly empty costs as much as a full one.
 template <class BlocksOf, class SmemOf>
-static int choose_tile(const void* kern, int T0, int ncomp, const FftPlan1D& pl, int maxb, int want, int maxthr, BlocksOf blocks_of,
+static int choose_tile(const void* kern, int T0, int ncomp, const FftPlan1D& pl, int rs, int want, int maxthr, BlocksOf blocks_of,
                        SmemOf smem_of, int& thr) {
     int best = -1, best_thr = 0;
     double best_cost = 0.0;
     for (int T = T0; T >= 1; T--) {
         int t = 0;
-        if (fit_tile(T, ncomp, pl, maxb, want, maxthr, t) != T) continue;
+        if (fit_tile(T, ncomp, pl, rs, want, maxthr, t) != T) continue;
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, t, smem_of(T)) != cudaSuccess || per_sm < 1) continue;
         const long long slots = (long long)per_sm * sm_count();
@@ -777,7 +795,7 @@ static int choose_tile(const void* kern, int T0, int ncomp, const FftPlan1D& pl,
             best_thr = t;
         }
     }
-    if (best < 0) return fit_tile(T0, ncomp, pl, maxb, want, maxthr, thr);
+    if (best < 0) return fit_tile(T0, ncomp, pl, rs, want, maxthr, thr);
     thr = best_thr;
     return best;
 }
@@ -787,7 +805,7 @@ static void green_apply_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& 
                            double* out, const double* c0, const double* s0, cudaStream_t st) {
     static const int mx = std::min(kernel_max_threads((const void*)k_green_x_fwd<RS>), kernel_max_threads((const void*)k_green_x_inv<RS>));
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, fft_maxb<RS>(), 256, mx, thr);
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, RS, 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
@@ -808,7 +826,7 @@ static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cu
     static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS, CT>);
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
-    const int G = choose_tile((const void*)k_fft_x_fwd<RS, CT>, x_rows_per_block(d.n1), 9, pl, fft_maxb<RS>(), 128, mx,
+    const int G = choose_tile((const void*)k_fft_x_fwd<RS, CT>, x_rows_per_block(d.n1), 9, pl, RS, 128, mx,
                               [&](int g) { return (npr + g - 1) / g; },
                               [&](int g) { return (size_t)9 * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
@@ -832,7 +850,7 @@ template <int RS, class CT>
 static void y_rs(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
     static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS, CT>), kernel_max_threads((const void*)k_fft_y<false, RS, CT>));
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_y<false, RS, CT>, y_tile(d), 1, pl, fft_maxb<RS>(), 64, mx,
+    const int T = choose_tile((const void*)k_fft_y<false, RS, CT>, y_tile(d), 1, pl, RS, 64, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n3 * ncomp; },
                               [&](int t) { return (size_t)t * d.n2 * sizeof(CT); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
@@ -855,7 +873,7 @@ template <int RS, class CT>
 static void z_green_rs(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS, CT>);
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_z_green<RS, CT>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+    const int T = choose_tile((const void*)k_fft_z_green<RS, CT>, z_tile(d), 9, pl, RS, 128, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
                               [&](int t) { return (size_t)9 * t * d.n3 * sizeof(CT); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
@@ -870,7 +888,7 @@ template <int RS>
 static void z_integ_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_integ<RS>);
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_z_integ<RS>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+    const int T = choose_tile((const void*)k_fft_z_integ<RS>, z_tile(d), 9, pl, RS, 128, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
                               [&](int t) { return (size_t)9 * t * d.n3 * sizeof(double2); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
@@ -886,7 +904,7 @@ template <int RS>
 static void z_grad_rs(const Dev& d, const FftPlan1D& pl, int ideriv, cudaStream_t st) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_grad<RS>);
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_z_grad<RS>, z_tile(d), 9, pl, fft_maxb<RS>(), 128, mx,
+    const int T = choose_tile((const void*)k_fft_z_grad<RS>, z_tile(d), 9, pl, RS, 128, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
                               [&](int t) { return (size_t)9 * t * d.n3 * sizeof(double2); }, thr);
     dim3 grid((d.n1h + T - 1) / T, d.n2);
@@ -898,7 +916,7 @@ static void gradient_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
                         double* out, int ideriv, cudaStream_t st) {
     static const int mx = std::min(kernel_max_threads((const void*)k_green_x_fwd<RS>), kernel_max_threads((const void*)k_green_x_inv<RS>));
     int thr = 0;
-    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, fft_maxb<RS>(), 256, mx, thr);
+    const int G = fit_tile(x_rows_per_block(d.n1), 9, pl1, RS, 256, mx, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     const int grid = (npairs + G - 1) / G;
     const size_t smem = (size_t)9 * G * d.n1 * sizeof(double2);
@@ -920,7 +938,7 @@ static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvPara
     const int ncomp = (mode == 0) ? 9 : 3;
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
-    const int G = choose_tile((const void*)k_fft_x_inv<RS, CT>, x_rows_per_block(d.n1), ncomp, pl, fft_maxb<RS>(), 128, mx,
+    const int G = choose_tile((const void*)k_fft_x_inv<RS, CT>, x_rows_per_block(d.n1), ncomp, pl, RS, 128, mx,
                               [&](int g) { return (npr + g - 1) / g; },
                               [&](int g) { return (size_t)ncomp * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
