@@ -334,11 +334,12 @@ def main(argv=None) -> int:
                 "kernel_share": {k: round(v[1] / max(sum(x[1] for x in kd.values()), 1e-30), 4) for k, v in
                                  sorted(kd.items(), key=lambda kv: -kv[1][1])}}
 
-    # end to end through the C ABI with host buffers: deck files -> device -> CSV rows (median of 3 runs)
+    # end to end through the C ABI with host buffers: deck files -> device -> CSV rows (median of 3 runs,
+    # after one untimed run of the same path that pays the one-time costs: output directory, device pool)
     e2e = None
     try:
         runs = []
-        for rep in range(3):
+        for rep in range(4):
             with tempfile.TemporaryDirectory() as td2:
                 fft2 = make_deck(Path(td2), n, args.steps + 1, args.ngrains)
                 out = Path(td2) / "out"
@@ -351,7 +352,8 @@ def main(argv=None) -> int:
                 s2.close()
                 torch.cuda.synchronize(dev)
                 we = time.perf_counter() - t0
-                runs.append((r2.voxel_iters / we, r2))
+                if rep > 0:
+                    runs.append((r2.voxel_iters / we, r2))
         runs.sort(key=lambda x: x[0])
         val, r2 = runs[1]
         e2e = {"value": val, "unit": METRIC,
@@ -359,7 +361,7 @@ def main(argv=None) -> int:
                "d2h_bytes_per_step": int(r2.d2h_bytes / max(args.steps, 1)),
                "runs": [round(x[0], 1) for x in runs],
                "note": "evp_open (deck files parsed and uploaded) + steps + results/diagnostics CSV rows, host wall "
-                       "clock; median of 3 runs"}
+                       "clock; median of 3 runs after one untimed run"}
     except Exception as exc:  # pragma: no cover - reported, not hidden
         e2e = {"value": None, "unit": METRIC, "error": str(exc)}
 

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <chrono>
 #include <mutex>
+#include <set>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
@@ -208,6 +209,23 @@ public:
         if (*h_err & 4) throw SolveError("form_G failed (singular acoustic tensor or complex D operator)", -3);
     }
 
+    // The solver allocates stream-ordered from the device's default memory pool.  By default
+    // that pool hands freed memory back to the driver at every synchronisation, so each new
+    // solve would map its ~5 kB per voxel afresh; keeping it in the pool makes back-to-back
+    // and concurrent solves reuse it (the memory stays with this process until it exits).
+    static void keep_pool_memory() {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return;
+        static std::mutex m;
+        static std::set<int> done;
+        std::lock_guard<std::mutex> lk(m);
+        if (!done.insert(dev).second) return;
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+
     // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
     void open(const std::string& fft_in, const std::string& out, int mix_flag, int modal_flag, int flags) {
         write_files = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) != 0;
@@ -234,6 +252,7 @@ public:
         CK(cudaEventCreate(&ev1));
         static std::once_flag configured;
         std::call_once(configured, [] { fft_configure(); });
+        keep_pool_memory();
         allocate();
         upload_and_init();
         modal = (modal_flag != 0);
