@@ -786,8 +786,42 @@ __device__ __forceinline__ double gsum6(double x, int base) {
 }
 __device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a > b ? a : b; }
 
+// Per-warp shared memory: rows of kXStride doubles, one double per lane (33 so that
+// lanes reading other lanes' entries hit distinct banks).
+constexpr int kXRows = 16, kXStride = 33;
+// N doubles owned by a lane: a column of the warp's shared memory (entries kXStride
+// apart) when SM, else registers (every index must then be a compile-time constant).
+template <bool SM, int N>
+struct LaneCol {
+    double* p;
+    double r[SM ? 1 : N];
+    __device__ __forceinline__ double& operator[](int i) {
+        if constexpr (SM) return p[i * kXStride];
+        else return r[i];
+    }
+};
+
+// Dynamic shared memory of k_newton6: with two systems per lane, per warp the lanes' Schmid
+// vectors (5 * SPL), rows of C~ and A (12), trial resistances (2 * SPL), slip rates, rate
+// factors, rate constants and exponents (4 * SPL) as columns; nothing with four per lane.
+__host__ __device__ constexpr bool newton6_cols_in_smem(int spl) { return spl == 2; }
+__host__ __device__ constexpr int newton6_col_rows(int spl) { return newton6_cols_in_smem(spl) ? 11 * spl + 12 : 0; }
+__host__ __device__ constexpr size_t newton6_smem_bytes(int spl) {
+    return 8 * sizeof(double) * (size_t)newton6_col_rows(spl) * kXStride;
+}
+
 template <int SPL, bool MODAL>
 __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
+    constexpr bool kSm = newton6_cols_in_smem(SPL);
+    extern __shared__ double dyn_smem[];
+    double* const col = dyn_smem + (threadIdx.x >> 5) * newton6_col_rows(SPL) * kXStride + (threadIdx.x & 31);
+    LaneCol<kSm, 6> Crow{col}, Arow{col + 6 * kXStride};             // rows r of C~ and A
+    LaneCol<kSm, 5 * SPL> SCH{col + 12 * kXStride};                  // Schmid vectors of the lane's systems
+    LaneCol<kSm, 2 * SPL> TT{col + (12 + 5 * SPL) * kXStride};       // trial resistances
+    LaneCol<kSm, SPL> GD{col + (12 + 7 * SPL) * kXStride};           // accepted slip rates
+    LaneCol<kSm, SPL> RS{col + (12 + 8 * SPL) * kXStride};           // and rate factors
+    LaneCol<kSm, SPL> G0{col + (12 + 9 * SPL) * kXStride};           // reference rates
+    LaneCol<kSm, SPL> NR{col + (12 + 10 * SPL) * kXStride};          // rate exponents
     const long long N = d.N;
     const int lane = threadIdx.x & 31;
     const int grp = lane / 6;               // 0..4 hold voxels; group 5 (lanes 30, 31) is idle
@@ -848,7 +882,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
             for (int c = 0; c < 6; c++) acc[8 + c] += s6v[c] * w;
         }
         // per-voxel vectors: full in every lane while A and q are formed, component r afterwards
-        double lam_r, sgt_r, D_r, eth_r, Crow[6], Arow[6], q_r;
+        double lam_r, sgt_r, D_r, eth_r, q_r;
         const PhaseDev& ph = d.ph[d.phase[v]];
         const int nsyst = ph.nsyst;
         {
@@ -902,21 +936,20 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
         eth_r = sel6(ethf, r);
         }
         // slip systems of this lane and their constants
-        double sch[SPL][5], tt[SPL][2], gd[SPL], rs1[SPL], g0s[SPL], nrs[SPL];
         double taun = 0.0;
 #pragma unroll
         for (int k = 0; k < SPL; k++) {
             const int s = r + 6 * k;
             const bool own = s < nsyst, any = s < d.nsys;
 #pragma unroll
-            for (int c = 0; c < 5; c++) sch[k][c] = own ? d.sch[(s * 5 + c) * N + v] : 0.0;
-            tt[k][0] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
-            tt[k][1] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
-            g0s[k] = own ? ph.gamd0[s] : 0.0;
-            nrs[k] = own ? ph.nrs[s] : 1.0;
-            gd[k] = 0.0;
-            rs1[k] = 0.0;
-            taun += tt[k][0] * tt[k][0] + tt[k][1] * tt[k][1];
+            for (int c = 0; c < 5; c++) SCH[5 * k + c] = own ? d.sch[(s * 5 + c) * N + v] : 0.0;
+            TT[2 * k] = any ? d.trialtau[(2 * s) * N + v] : 0.0;
+            TT[2 * k + 1] = any ? d.trialtau[(2 * s + 1) * N + v] : 0.0;
+            G0[k] = own ? ph.gamd0[s] : 0.0;
+            NR[k] = own ? ph.nrs[s] : 1.0;
+            GD[k] = 0.0;
+            RS[k] = 0.0;
+            taun += TT[2 * k] * TT[2 * k] + TT[2 * k + 1] * TT[2 * k + 1];
         }
         const int int_exp = ph.int_exp;
         taun = sqrt(gsum6(taun, base));
@@ -954,15 +987,15 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
                         gdn[k] = 0.0;
                         rsn[k] = 0.0;
                         if (r + 6 * k < nsyst) {
-                            double rss = sch[k][0] * sgf[0] + sch[k][1] * sgf[1] + sch[k][2] * sgf[2] + sch[k][3] * sgf[3] +
-                                         sch[k][4] * sgf[4];
-                            const double tau = (rss - 0.0 < 0.0) ? tt[k][1] : tt[k][0];
+                            double rss = SCH[5 * k + 0] * sgf[0] + SCH[5 * k + 1] * sgf[1] + SCH[5 * k + 2] * sgf[2] + SCH[5 * k + 3] * sgf[3] +
+                                         SCH[5 * k + 4] * sgf[4];
+                            const double tau = (rss - 0.0 < 0.0) ? TT[2 * k + 1] : TT[2 * k];
                             rss = (rss - 0.0) / tau;
-                            const double dum = g0s[k] * powabs(rss, nrs[k] - 1.0, int_exp);
-                            rsn[k] = nrs[k] * dum / tau;
+                            const double dum = G0[k] * powabs(rss, NR[k] - 1.0, int_exp);
+                            rsn[k] = NR[k] * dum / tau;
                             gdn[k] = rss * dum;
 #pragma unroll
-                            for (int c = 0; c < 5; c++) ep[c] += sch[k][c] * gdn[k];
+                            for (int c = 0; c < 5; c++) ep[c] += SCH[5 * k + c] * gdn[k];
                         }
                     }
                     double rn = -q_r, epr = 0.0;
@@ -978,8 +1011,8 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
                     if (aC) {
 #pragma unroll
                         for (int k = 0; k < SPL; k++) {
-                            gd[k] = gdn[k];
-                            rs1[k] = rsn[k];
+                            GD[k] = gdn[k];
+                            RS[k] = rsn[k];
                         }
                         edotp_r = epr;
                         sev_r = sg_r;
@@ -1005,7 +1038,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
 #pragma unroll
                         for (int jj = 0; jj < 5; jj++)
 #pragma unroll
-                            for (int ii = 0; ii <= jj; ii++) dd[q++] += sch[k][ii] * sch[k][jj] * rs1[k];
+                            for (int ii = 0; ii <= jj; ii++) dd[q++] += SCH[5 * k + ii] * SCH[5 * k + jj] * RS[k];
                     }
                 }
 #pragma unroll
@@ -1075,14 +1108,14 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
                 double dg = 0.0;
 #pragma unroll
                 for (int k = 0; k < SPL; k++)
-                    if (r + 6 * k < nsyst) dg += fabs(gd[k]) * p.tdot;
+                    if (r + 6 * k < nsyst) dg += fabs(GD[k]) * p.tdot;
                 const double deltgam = gsum6(dg, base);
                 const double gamma1 = gamma0 + deltgam;
                 double gall[6 * SPL];
 #pragma unroll
                 for (int k = 0; k < SPL; k++)
 #pragma unroll
-                    for (int q = 0; q < 6; q++) gall[6 * k + q] = fabs(__shfl_sync(kFull, gd[k], base + q));
+                    for (int q = 0; q < 6; q++) gall[6 * k + q] = fabs(__shfl_sync(kFull, GD[k], base + q));
                 double e2 = 0.0, tn[SPL][2];
 #pragma unroll
                 for (int k = 0; k < SPL; k++) {
@@ -1107,14 +1140,14 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
                         tn[k][0] = d.crss[(2 * s) * N + v] + dtau * voce * p.tdot / deltgam;
                         tn[k][1] = d.crss[(2 * s + 1) * N + v] + dtau * voce * p.tdot / deltgam;
                     }
-                    e2 += (tt[k][0] - tn[k][0]) * (tt[k][0] - tn[k][0]) + (tt[k][1] - tn[k][1]) * (tt[k][1] - tn[k][1]);
+                    e2 += (TT[2 * k] - tn[k][0]) * (TT[2 * k] - tn[k][0]) + (TT[2 * k + 1] - tn[k][1]) * (TT[2 * k + 1] - tn[k][1]);
                 }
                 const double et = sqrt(gsum6(e2, base)) / taun;
                 if (aT) {
 #pragma unroll
                     for (int k = 0; k < SPL; k++) {
-                        tt[k][0] = tn[k][0];
-                        tt[k][1] = tn[k][1];
+                        TT[2 * k] = tn[k][0];
+                        TT[2 * k + 1] = tn[k][1];
                     }
                     errtau = et;
                 }
@@ -1151,9 +1184,9 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
             for (int k = 0; k < SPL; k++) {
                 const int s = r + 6 * k;
                 if (s < d.nsys) {
-                    d.gamdot[s * N + v] = (s < nsyst) ? gd[k] : 0.0;
-                    d.trialtau[(2 * s) * N + v] = tt[k][0];
-                    d.trialtau[(2 * s + 1) * N + v] = tt[k][1];
+                    d.gamdot[s * N + v] = (s < nsyst) ? GD[k] : 0.0;
+                    d.trialtau[(2 * s) * N + v] = TT[2 * k];
+                    d.trialtau[(2 * s + 1) * N + v] = TT[2 * k + 1];
                 }
             }
             if (r == 0) {
@@ -1177,7 +1210,6 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
 // one double per lane at a stride of 33 doubles, so that lanes reading another
 // lane's entries hit distinct banks.  Every write phase starts with
 // __syncwarp(), so a row is never overwritten before all lanes have read it.
-constexpr int kXRows = 16, kXStride = 33;
 struct Xw {
     double* P;      // [kXRows][kXStride]; row kXRows - 1 serves the scalar sums and gathers
     int lane, base;
@@ -1212,17 +1244,6 @@ struct PhaseN {
 };
 constexpr int kMaxPhaseSmem = 4;
 
-// N doubles owned by a lane: a column of the warp's shared memory (entries kXStride
-// apart) when SM, else registers (every index must then be a compile-time constant).
-template <bool SM, int N>
-struct LaneCol {
-    double* p;
-    double r[SM ? 1 : N];
-    __device__ __forceinline__ double& operator[](int i) {
-        if constexpr (SM) return p[i * kXStride];
-        else return r[i];
-    }
-};
 
 // Dynamic shared memory of k_newton6p: the staged phases, then per warp the
 // exchange rows, the lanes' columns (rows of kXStride doubles) and the five
@@ -1716,12 +1737,19 @@ void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
         }
         return;
     }
+    const size_t sm6 = newton6_smem_bytes(big ? 4 : 2);
     if (p.modal) {
-        if (big) k_newton6<4, true><<<grid, 256, 0, st>>>(d, p);
-        else k_newton6<2, true><<<grid, 256, 0, st>>>(d, p);
+        if (big) k_newton6<4, true><<<grid, 256, sm6, st>>>(d, p);
+        else {
+            cudaFuncSetAttribute(k_newton6<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
+            k_newton6<2, true><<<grid, 256, sm6, st>>>(d, p);
+        }
     } else {
-        if (big) k_newton6<4, false><<<grid, 256, 0, st>>>(d, p);
-        else k_newton6<2, false><<<grid, 256, 0, st>>>(d, p);
+        if (big) k_newton6<4, false><<<grid, 256, sm6, st>>>(d, p);
+        else {
+            cudaFuncSetAttribute(k_newton6<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
+            k_newton6<2, false><<<grid, 256, sm6, st>>>(d, p);
+        }
     }
 }
 
