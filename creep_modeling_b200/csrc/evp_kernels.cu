@@ -1281,8 +1281,9 @@ __host__ __device__ constexpr size_t newton6p_smem_bytes(int spl, int nph) {
 // 0..5 (Gauss-Jordan), and lane r ends with the unknown of column r; lane r
 // reads only row r of dd.  Against dgesv on J the Newton step differs in
 // rounding only.  Five voxels per warp, six lanes per voxel as in k_newton6;
-// the Schmid vectors, resistances and the per-group sums live in shared
-// memory, which keeps the kernel within 128 registers (16 warps per SM).
+// the Schmid vectors, the per-group sums and (two systems per lane) the lane's
+// operator rows and per-system state live in shared memory, which keeps the
+// kernel within 128 registers with few spills (16 warps per SM).
 template <int SPL>
 __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     constexpr int MS = 6 * SPL;
@@ -1333,7 +1334,6 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     __syncwarp();
     double* const accg = accw + (grp < 5 ? grp : 0) * 14;
     const double tolt = fmax(p.error, p.erroral);
-    // position of dd(r, j) in the packed upper triangle, for this lane's row
     const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long v0 = wid * 5; v0 < N; v0 += nwarp * 5) {  // warp-uniform
