@@ -60,3 +60,19 @@ def test_mixed_precision_curves_and_fields(tmp_path):
     ferr = float(np.max(np.abs(vm32 - vm64)) / np.max(vm64))
     print("von Mises field error:", ferr)
     assert ferr <= FIELD_TOL
+
+
+@pytest.mark.parametrize("igamma", [1, 2])
+def test_mixed_precision_discrete_green(tmp_path, igamma):
+    """The tabulated IGAMMA 1 / 2 operator read into the FP32 Green step: same bars."""
+    case = decks.case_c3(stress33=150.0, nsteps=4, n=16, ngrains=20)
+    case.processes[0].igamma = igamma
+    fft = decks.write_case(case, tmp_path)
+    r64, sg64 = _run(fft, 0, 4)
+    r32, sg32 = _run(fft, 1, 4)
+    for grp in RESULT_GROUPS:
+        scale = np.max(np.abs(r64[:, grp]))
+        if scale >= 1e-30:
+            assert np.max(np.abs(r32[:, grp] - r64[:, grp])) / scale <= CURVE_TOL, grp
+    vm64, vm32 = _vm(sg64), _vm(sg32)
+    assert np.max(np.abs(vm32 - vm64)) / np.max(vm64) <= FIELD_TOL

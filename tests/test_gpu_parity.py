@@ -178,16 +178,18 @@ def test_discrete_green_operator_odd_grid_parity(tmp_path, igamma):
 def test_initial_displacement_parity(tmp_path, kind):
     """IDISPINI 1 (displacement at cell centres, nodes by averaging, central-difference gradient)
     and 2 (at nodes, rotated-scheme gradient): F = grad u + diag(4) (the reference forces delt = 4),
-    F_ini = F in the elastic update, weights w det F / <det F>, shifted node coordinates."""
-    for case in (decks.case_c1(nsteps=3), decks.case_c2(nsteps=3, n=12, ngrains=12)):
+    F_ini = F in the elastic update, weights w det F / <det F>, shifted node coordinates; creep also
+    with the modified augmented Lagrangian (its operator is pulled back with the initial F)."""
+    for case, modal in ((decks.case_c1(nsteps=3), 0), (decks.case_c2(nsteps=3, n=12, ngrains=12), 0),
+                        (decks.case_c1(nsteps=3), 1)):
         case.n = 12
         case.ngrains = 12
         case.dispini = kind
-        fft = decks.write_case(case, tmp_path / case.name)
-        g, o, rg, ro, dg, do = parity.run_both(fft, 3)
+        fft = decks.write_case(case, tmp_path / f"{case.name}_m{modal}")
+        g, o, rg, ro, dg, do = parity.run_both(fft, 3, mix=1, modal=modal)
         parity.assert_rows_match(rg, ro, dg, do)
         for f in FIELDS:
-            assert parity.field_rel_err(g, o, f) <= parity.RTOL, (case.name, f)
+            assert parity.field_rel_err(g, o, f) <= parity.RTOL, (case.name, modal, f)
 
 
 def test_two_dimensional_grid_parity(tmp_path):
