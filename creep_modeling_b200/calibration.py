@@ -178,12 +178,19 @@ def srj_objective(results, target: SrjTarget, metric: str = "MAE", align: str = 
 
 
 def read_results(out_dir) -> dict:
-    """The results.csv columns the objectives use, as float arrays."""
+    """The results.csv columns the objectives use, as float arrays, cut before the first
+    diverged increment (non-finite eav33, sav33 or epav33), as SimResults.load does
+    (data_utils.py:261-296)."""
     import pandas as pd
 
     df = pd.read_csv(Path(out_dir) / "results.csv")
     df.columns = df.columns.str.strip()
-    return {c: df[c].to_numpy(dtype=float) for c in ("iter", "sim_time", "epav33", "sav33", "eav33")}
+    out = {c: df[c].to_numpy(dtype=float) for c in ("iter", "sim_time", "epav33", "sav33", "eav33")}
+    ok = np.isfinite(out["eav33"]) & np.isfinite(out["sav33"]) & np.isfinite(out["epav33"])
+    bad = np.where(~ok)[0]
+    if len(bad) > 0:
+        out = {c: a[: bad[0]] for c, a in out.items()}
+    return out
 
 
 # ---------------------------------------------------------------- the batch

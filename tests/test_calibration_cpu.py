@@ -113,3 +113,13 @@ def test_evaluate_batch_submits_everything_before_waiting(tmp_path):
     assert res[0]["loss"] == pytest.approx(0.01 * res[0]["avg_iters"], rel=1e-9)
     assert res[1]["base"] > 0.0
     assert res[2]["status"] == -5 and res[2]["loss"] == np.inf
+
+
+def test_read_results_stops_at_the_first_diverged_increment(tmp_path):
+    import pandas as pd
+
+    pd.DataFrame({"iter": [3, 4, 5, 6], "sim_time": [1.0, 2.0, 3.0, 4.0], "epav33": [1e-6, 2e-6, float("nan"), 4e-6],
+                  "sav33": [100.0, 100.0, 100.0, 100.0], "eav33": [1e-3, 1e-3, 1e-3, 1e-3]}).to_csv(tmp_path / "results.csv",
+                                                                                            index=False)
+    r = cal.read_results(tmp_path)
+    assert list(r["sim_time"]) == [1.0, 2.0] and list(r["iter"]) == [3.0, 4.0]
