@@ -54,7 +54,32 @@ def algorithmic_bytes(n1: int, nsys: int = 12) -> dict:
     }
 
 
-LAUNCHES_PER_RECORD = {"k_grid_fft": 5}
+# Counted FP64 arithmetic of k_newton6p (12 slip systems; a fused multiply-add counts 2, a division
+# 1, the integer power |x|^(n-1) by binary powering 8): one constitutive evaluation (resolved shear,
+# power law, plastic strain rate, residual rho and C~ rho, their norm) 612; one Newton step (the
+# tangent dd, the rows of H, Gauss-Jordan on the 6x6 system, the update and its norm) 1000; one
+# hardening update (Voce increment, the 12 x 12 latent-hardening product, the resistance change) 780.
+NEWTON_FLOPS = {"evaluation": 612, "newton_step": 1000, "hardening_update": 780}
+
+
+def fp64_peak_tflops(dev) -> float:
+    """Measured FP64 rate of this GPU: cuBLAS DGEMM (torch float64 matmul, 8192^3), best of 5."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 0.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(5):
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
 
 
 def load_peaks() -> tuple[float, str]:
@@ -124,13 +149,20 @@ def make_deck(root: Path, n: int, nsteps: int, ngrains: int) -> Path:
     return decks.write_case(case, root)
 
 
-def cpu_baseline(fft: Path, nmacro: int, budget_s: float) -> dict:
-    """The oracle on all host cores, on a bounded sample of the same workload."""
+WORKLOAD = "tension {n}^3, {g} grains, n=20, udot33=1e-3/s, dt=0.5 s, iupdate=1"
+
+
+def cpu_baseline(fft: Path, warmup: int, nmacro: int, budget_s: float) -> dict:
+    """The oracle on all host cores, on a bounded sample of the same workload: the increments
+    after the warm-up ones, as the device figure times them, until nmacro are done or
+    budget_s of timed CPU work has passed."""
     import oracle
 
     threads = os.cpu_count() or 1
     s = oracle.OracleSolve(fft, mix=1, modal=0, nthreads=threads)
-    done = iters0 = 0
+    for _ in range(warmup):
+        s.advance(1)
+    done = 0
     iters0 = s.total_iters()
     t0 = time.perf_counter()
     while done < nmacro:
@@ -143,7 +175,8 @@ def cpu_baseline(fft: Path, nmacro: int, budget_s: float) -> dict:
     vi = (s.total_iters() - iters0) * s.nvox
     s.close()
     return {"value": vi / dt, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"first {done} increment(s) of the same {s.shape[0]}^3 tension deck ({vi} voxel-iters, {dt:.1f} s)"}
+            "sample": f"increments {warmup + 1}-{warmup + done} of the same {s.shape[0]}^3 tension deck "
+                      f"({vi} voxel-iters, {dt:.1f} s)"}
 
 
 def run_reference(args, ws, rank):
@@ -158,12 +191,8 @@ def run_reference(args, ws, rank):
         s = oracle.OracleSolve(fft, mix=1, modal=0, nthreads=threads)
         budget = args.ref_budget
         t_all = time.perf_counter()
-        wdone = 0
-        for _ in range(args.warmup):
-            if time.perf_counter() - t_all > budget / 3:
-                break
+        for _ in range(args.warmup):  # the same untimed increments as the device arm
             s.advance(1)
-            wdone += 1
         it0 = s.total_iters()
         t0 = time.perf_counter()
         done = 0
@@ -175,17 +204,47 @@ def run_reference(args, ws, rank):
         dt = time.perf_counter() - t0
         vi = (s.total_iters() - it0) * s.nvox
         value = vi / dt
-        sample = (f"{done} timed increment(s) after {wdone} warm-up of the {n}^3 tension deck on {threads} host threads "
-                  f"(C++ FP64 restatement of the reference Fortran solver)")
+        sample = (f"increments {args.warmup + 1}-{args.warmup + done} (after {args.warmup} untimed) of the {n}^3 "
+                  f"tension deck on {threads} host threads (C++ FP64 restatement of the reference Fortran solver)")
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": done,
-                "warmup": wdone, "ms_per_step": dt / max(done, 1) * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"tension {n}^3, 500 grains, n=20, udot33=1e-3/s, dt=0.5 s, iupdate=1",
-                           "voxels": n ** 3, "l2": "state larger than L2"},
+                "warmup": args.warmup, "ms_per_step": dt / max(done, 1) * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD.format(n=n, g=args.ngrains), "voxels": n ** 3,
+                           "increments_timed": f"{args.warmup + 1}-{args.warmup + done}",
+                           "l2": "state larger than L2"},
                 "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
                 "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
     return 0
+
+
+def fft_vs_cufft(kd: dict, iters: int, n: int, dev) -> dict:
+    """The five FFT passes of one equilibrium iteration (PK1 prologue, x R2C, y, z with the
+    Green-operator product, y inverse, x C2R with the correction epilogue; their average
+    device time per iteration from the profiled increments) beside cuFFT (through
+    torch.fft) doing only the real-to-complex and complex-to-real 3-D transforms of the
+    same nine FP64 fields, timed with CUDA events.  A timing comparison, not a product path."""
+    import torch
+
+    ours = sum(kd.get(k, (0, 0.0))[1] for k in ("k_fft_x_fwd", "k_fft_y_fwd", "k_fft_z_green", "k_fft_y_inv",
+                                                 "k_fft_x_inv")) / max(iters, 1)
+    x = torch.randn(9, n, n, n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        y = torch.fft.irfftn(torch.fft.rfftn(x, dim=(1, 2, 3)), s=(n, n, n), dim=(1, 2, 3))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    torch.cuda.synchronize(dev)
+    a.record()
+    for _ in range(reps):
+        y = torch.fft.irfftn(torch.fft.rfftn(x, dim=(1, 2, 3)), s=(n, n, n), dim=(1, 2, 3))
+    b.record()
+    torch.cuda.synchronize(dev)
+    cu = a.elapsed_time(b) / reps
+    del y
+    return {"grid": f"{n}^3 x 9 fields FP64", "ours_five_passes_ms": ours, "cufft_r2c_c2r_ms": cu,
+            "ratio_cufft_over_ours": cu / ours if ours else None,
+            "note": "ours includes the PK1 prologue, the Green-operator product and the correction epilogue; "
+                    "cuFFT does the transforms only (torch.fft)"}
 
 
 def serving_sample(k: int, scale: float, rate: float) -> dict:
@@ -230,14 +289,15 @@ def serving_sample(k: int, scale: float, rate: float) -> dict:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=64, help="grid edge (default: the 64^3 configuration)")
     ap.add_argument("--ngrains", type=int, default=500)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--cpu-steps", type=int, default=1)
-    ap.add_argument("--ref-budget", type=float, default=150.0, help="seconds of CPU time for --impl reference")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the cpu_baseline leg")
+    ap.add_argument("--ref-budget", type=float, default=300.0, help="seconds of CPU time for --impl reference")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests in the served-stream sample (0: skip)")
     ap.add_argument("--serve-scale", type=float, default=0.1, help="increment-count scale of the served-stream sample")
     args = ap.parse_args(argv)
@@ -265,7 +325,9 @@ def main(argv=None) -> int:
     n = args.n
     td = tempfile.mkdtemp(prefix=f"evp_bench_r{rank}_")
     fft = make_deck(Path(td), n, args.warmup + args.steps + 1, args.ngrains)
-    s = Solve(fft, mix=1, modal=0, profile=True)
+
+    # 1. the device figure: increments W+1..W+K, CUDA events on the solver's stream, no per-kernel timers
+    s = Solve(fft, mix=1, modal=0)
     for _ in range(args.warmup):
         s.advance(1)
     clocks = ClockSampler(local if ws > 1 else 0)
@@ -273,7 +335,7 @@ def main(argv=None) -> int:
         pg.barrier()
     torch.cuda.synchronize(dev)
     st0 = s.stats()
-    kt0 = s.kernel_times()
+    l0 = s.launches()
     clocks.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -284,9 +346,10 @@ def main(argv=None) -> int:
     if pg:
         pg.barrier()
     st1 = s.stats()
-    kt1 = s.kernel_times()
+    launches = s.launches() - l0
+    s.close()
     gpu_s = st1.gpu_s - st0.gpu_s
-    vi = (st1.equilibrium_iters - st0.equilibrium_iters) * s.nvox
+    vi = (st1.equilibrium_iters - st0.equilibrium_iters) * (n ** 3)
     iters = st1.equilibrium_iters - st0.equilibrium_iters
     if pg:
         t = torch.tensor([gpu_s, float(vi)], dtype=torch.float64, device=dev)
@@ -297,21 +360,66 @@ def main(argv=None) -> int:
     else:
         gpu_s_max, vi_tot = gpu_s, float(vi)
     value = vi_tot / gpu_s_max
-    # per-kernel device time in the timed region
+
+    # 2. end to end through the C ABI on the same increments: a second solve of the same deck
+    #    writing results.csv and diagnostics.csv, host wall clock around its K increments (every
+    #    increment uploads its reference-medium constants and reads its sums and rows back)
+    e2e = None
+    try:
+        out = Path(td) / "e2e_out"
+        s2 = Solve(fft, out_dir=out, mix=1, modal=0, csv_only=True)
+        for _ in range(args.warmup):
+            s2.advance(1)
+        r0 = s2.stats()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s2.advance(1)
+        torch.cuda.synchronize(dev)
+        we = time.perf_counter() - t0
+        r1 = s2.stats()
+        s2.close()
+        vi2 = (r1.equilibrium_iters - r0.equilibrium_iters) * (n ** 3)
+        e2e = {"value": vi2 / we, "unit": METRIC,
+               "h2d_bytes_per_step": int((r1.h2d_bytes - r0.h2d_bytes) / max(args.steps, 1)),
+               "d2h_bytes_per_step": int((r1.d2h_bytes - r0.d2h_bytes) / max(args.steps, 1)),
+               "increments": f"{args.warmup + 1}-{args.warmup + args.steps}",
+               "same_iterations_as_device": bool(vi2 == vi),
+               "note": "evp_advance through the C ABI with results/diagnostics CSV written, host wall clock"}
+        # the whole solve as a caller runs it: deck files -> evp_solve_file -> output files
+        from creep_modeling_b200 import solver as _solver
+
+        t0 = time.perf_counter()
+        rep = _solver.run_solver(fft, Path(td) / "whole_out", mix=1, modal=0)
+        wt = time.perf_counter() - t0
+        e2e["whole_solve"] = {"value": rep.voxel_iters / wt, "unit": METRIC, "increments": rep.macrosteps,
+                              "wall_s": wt, "note": "evp_solve_file: deck parse + upload + every increment + "
+                                                    "results, diagnostics and VTK files"}
+    except Exception as exc:  # pragma: no cover - reported, not hidden
+        e2e = {"value": None, "unit": METRIC, "error": str(exc)}
+
+    # 3. per-kernel device times on the same increments of a third, profiled solve (an event pair
+    #    around every launch): the roofline of the dominant kernel and the kernel shares
+    sp = Solve(fft, mix=1, modal=0, profile=True)
+    for _ in range(args.warmup):
+        sp.advance(1)
+    kt0, p0, ns0 = sp.kernel_times(), sp.stats(), sp.newton_stats()
+    for _ in range(args.steps):
+        sp.advance(1)
+    kt1, p1, ns1 = sp.kernel_times(), sp.stats(), sp.newton_stats()
+    sp.close()
+    nst = {k: ns1[k] - ns0[k] for k in ns1}
     kd = {}
-    launches = 0
     for k, (cnt, ms) in kt1.items():
         c0, m0 = kt0.get(k, (0, 0.0))
         kd[k] = (cnt - c0, ms - m0)
-        launches += (cnt - c0) * LAUNCHES_PER_RECORD.get(k, 1)
-    s.close()
+    piters = p1.equilibrium_iters - p0.equilibrium_iters
 
     if rank != 0:
         if pg:
             pg.destroy_process_group()
         return 0
 
-    # roofline of the dominant kernel
     peak, peak_kind = load_peaks()
     ab = algorithmic_bytes(n)
     dom = max(kd, key=lambda k: kd[k][1]) if kd else None
@@ -331,46 +439,41 @@ def main(argv=None) -> int:
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": (ach / peak if ach else None), "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
                 "avg_launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": bytes_launch,
+                "timing": "CUDA events around each launch in a separate profiled solve over the same increments",
                 "kernel_share": {k: round(v[1] / max(sum(x[1] for x in kd.values()), 1e-30), 4) for k, v in
                                  sorted(kd.items(), key=lambda kv: -kv[1][1])}}
-
-    # end to end through the C ABI with host buffers: deck files -> device -> CSV rows (median of 3 runs,
-    # after one untimed run of the same path that pays the one-time costs: output directory, device pool)
-    e2e = None
-    try:
-        runs = []
-        for rep in range(4):
-            with tempfile.TemporaryDirectory() as td2:
-                fft2 = make_deck(Path(td2), n, args.steps + 1, args.ngrains)
-                out = Path(td2) / "out"
-                torch.cuda.synchronize(dev)
-                t0 = time.perf_counter()
-                s2 = Solve(fft2, out_dir=out, mix=1, modal=0, csv_only=True)
-                for _ in range(args.steps):
-                    s2.advance(1)
-                r2 = s2.stats()
-                s2.close()
-                torch.cuda.synchronize(dev)
-                we = time.perf_counter() - t0
-                if rep > 0:
-                    runs.append((r2.voxel_iters / we, r2))
-        runs.sort(key=lambda x: x[0])
-        val, r2 = runs[1]
-        e2e = {"value": val, "unit": METRIC,
-               "h2d_bytes_per_step": int(r2.h2d_bytes / max(args.steps, 1)),
-               "d2h_bytes_per_step": int(r2.d2h_bytes / max(args.steps, 1)),
-               "runs": [round(x[0], 1) for x in runs],
-               "note": "evp_open (deck files parsed and uploaded) + steps + results/diagnostics CSV rows, host wall "
-                       "clock; median of 3 runs after one untimed run"}
-    except Exception as exc:  # pragma: no cover - reported, not hidden
-        e2e = {"value": None, "unit": METRIC, "error": str(exc)}
+        if dom == "k_newton" and nst.get("eval_passes"):
+            flops = (nst["evaluations"] * NEWTON_FLOPS["evaluation"] + nst["newton_steps"] * NEWTON_FLOPS["newton_step"]
+                     + nst["hardening_updates"] * NEWTON_FLOPS["hardening_update"])
+            try:
+                fpk = fp64_peak_tflops(dev)
+            except Exception:  # pragma: no cover
+                fpk = None
+            ach_tf = flops / (ms / 1e3) / 1e12
+            roof["fp64"] = {
+                "counted_flops_per_launch": flops / max(cnt, 1), "achieved_tflops": ach_tf,
+                "peak_tflops": fpk, "peak_source": "measured cuBLAS DGEMM (torch float64 matmul 8192^3)",
+                "frac": (ach_tf / fpk if fpk else None), "flops_model": NEWTON_FLOPS,
+                "per_voxel": {"evaluations": nst["evaluations"] / max(nst["voxels"], 1),
+                              "newton_steps": nst["newton_steps"] / max(nst["voxels"], 1),
+                              "hardening_updates": nst["hardening_updates"] / max(nst["voxels"], 1)},
+                "active_slot_fraction": nst["evaluations"] / (5.0 * nst["eval_passes"]),
+                "active_slot_fraction_newton": nst["newton_steps"] / (5.0 * max(nst["newton_passes"], 1)),
+                "note": "voxel slots: five six-lane groups per warp; a slot idles while the warp waits for its "
+                        "slowest voxel"}
 
     cpu = None
     if not args.no_cpu:
         try:
-            cpu = cpu_baseline(fft, args.cpu_steps, 60.0)
+            cpu = cpu_baseline(fft, args.warmup, args.cpu_steps, args.cpu_budget)
         except Exception as exc:  # pragma: no cover
             cpu = {"value": None, "error": str(exc)}
+
+    fftcmp = None
+    try:
+        fftcmp = fft_vs_cufft(kd, piters, n, dev)
+    except Exception as exc:  # pragma: no cover
+        fftcmp = {"error": str(exc)}
 
     serving = None
     if args.serve_requests > 0:
@@ -383,11 +486,11 @@ def main(argv=None) -> int:
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": gpu_s_max / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"tension {n}^3, {args.ngrains} grains, n=20, udot33=1e-3/s, dt=0.5 s, iupdate=1 "
-                               "(plain FP64)", "voxels": n ** 3, "equilibrium_iters": int(iters),
+        "config": {"workload": WORKLOAD.format(n=n, g=args.ngrains), "voxels": n ** 3, "equilibrium_iters": int(iters),
+                   "increments_timed": f"{args.warmup + 1}-{args.warmup + args.steps}", "precision": "plain FP64",
                    "parallelism": f"replicas x{ws}", "l2": "state (~460 MB) larger than L2; no flush"},
         "wall_s": wall, "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-        "serving": serving,
+        "fft_vs_cufft": fftcmp, "serving": serving,
     }
     print(json.dumps(line), flush=True)
     if pg:

@@ -12,13 +12,14 @@ LIB_PATH = Path(__file__).resolve().parent / "_build" / "libevp_b200.so"
 EXPORTED = (
     "evp_solve_file", "evp_open", "evp_advance", "evp_get_field", "evp_last_rows", "evp_stats", "evp_close",
     "evp_kernel_times", "evp_green_apply", "evp_green_apply_noalloc", "evp_last_error", "evp_version",
-    "evp_server_open", "evp_submit", "evp_poll", "evp_wait", "evp_server_close",
+    "evp_server_open", "evp_submit", "evp_submit_deadline", "evp_poll", "evp_wait", "evp_server_close",
+    "evp_set_deadline", "evp_kernel_launches", "evp_newton_stats",
 )
 
 STATUS = {
     0: "ok", -1: "deck or input-file error", -2: "deck feature not supported", -3: "singular matrix",
     -4: "non-convergence or non-finite state", -5: "output-file error", -6: "CUDA error or no device",
-    -7: "bad argument",
+    -7: "bad argument", -8: "deadline exceeded",
 }
 
 
@@ -96,6 +97,10 @@ def load(path: Path | str | None = None):
     L.evp_close.restype = ctypes.c_int
     L.evp_kernel_times.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong), c_dp, ctypes.c_int]
     L.evp_kernel_times.restype = ctypes.c_int
+    L.evp_newton_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.evp_newton_stats.restype = ctypes.c_int
+    L.evp_kernel_launches.argtypes = [vp]
+    L.evp_kernel_launches.restype = ctypes.c_longlong
     L.evp_green_apply.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, vp]
     L.evp_green_apply.restype = ctypes.c_int
     L.evp_green_apply_noalloc.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, vp]
@@ -110,6 +115,11 @@ def load(path: Path | str | None = None):
     L.evp_submit.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                              ctypes.POINTER(u64)]
     L.evp_submit.restype = ctypes.c_int
+    L.evp_submit_deadline.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_double, ctypes.POINTER(u64)]
+    L.evp_submit_deadline.restype = ctypes.c_int
+    L.evp_set_deadline.argtypes = [vp, ctypes.c_double]
+    L.evp_set_deadline.restype = ctypes.c_int
     L.evp_poll.argtypes = [vp, u64, ctypes.POINTER(Status)]
     L.evp_poll.restype = ctypes.c_int
     L.evp_wait.argtypes = [vp, u64, ctypes.c_double, ctypes.POINTER(Status)]

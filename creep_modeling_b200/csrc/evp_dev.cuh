@@ -85,6 +85,10 @@ struct Dev {
     double* Fini;  // initial deformation gradient (IDISPINI 1, 2 only; null: identity)
     // reductions
     double *partials, *red;
+    // Newton activity counters (null unless the solve is profiled): [0] warp passes of the
+    // evaluation loop, [1] voxel evaluations done in them, [2] Newton steps, [3] hardening
+    // updates, [4] voxels, [5] warp passes of the Newton-step loop
+    unsigned long long* nstats;
     unsigned int *counters;
     int *err;  // error word: bit 0 singular matrix, bit 1 non-finite Newton result, bit 2 form_G failure
     const PhaseDev *ph;

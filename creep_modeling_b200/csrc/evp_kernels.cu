@@ -1336,6 +1336,9 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     const double tolt = fmax(p.error, p.erroral);
     const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const bool stats = d.nstats != nullptr;
+    unsigned long long c_pass = 0, c_eval = 0, c_nr = 0, c_tau = 0, c_vox = 0, c_npass = 0;  // warp-uniform counts
+    const unsigned lead = 0x01041041u;  // lanes 0, 6, 12, 18, 24: one per voxel group
     for (long long v0 = wid * 5; v0 < N; v0 += nwarp * 5) {  // warp-uniform
         const bool valid = grp < 5 && v0 + grp < N;
         const long long v = valid ? v0 + grp : v0;  // in-range index for the loads of idle lanes
@@ -1408,9 +1411,11 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
         int itertau = 0;
         double errtau = 2.0 * tolt;
         bool aT = act;
+        if (stats) c_vox += __popc(__ballot_sync(kFull, act) & lead);
         while (true) {
             aT = aT && itertau < 10 && errtau > tolt;
             if (!__any_sync(kFull, aT)) break;
+            if (stats) c_tau += __popc(__ballot_sync(kFull, aT) & lead);
             itertau += aT;
             // residual norms and the Newton correction are compared as squares (no square roots
             // on the iteration's critical path): resn2 = |res|^2, and the loop runs while
@@ -1423,6 +1428,10 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
             while (true) {
                 aN = aN && iterNR < 100 && more;
                 if (!__any_sync(kFull, aN)) break;
+                if (stats) {
+                    c_nr += __popc(__ballot_sync(kFull, aN) & lead);
+                    c_npass++;
+                }
                 iterNR += aN;
                 int icut = 0;
                 double resn2 = 4.0 * resoldn2, rho_c = 0.0;
@@ -1430,6 +1439,10 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
                 while (true) {
                     aC = aC && resn2 > resoldn2 && icut < 10;
                     if (!__any_sync(kFull, aC)) break;
+                    if (stats) {
+                        c_eval += __popc(__ballot_sync(kFull, aC) & lead);
+                        c_pass++;
+                    }
                     // plastic_strain_rate at sg (own systems)
                     double sgf[6];
                     xgather(X, sg_r, sgf);
@@ -1703,6 +1716,14 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
         }
     }
     __syncwarp();
+    if (stats && lane == 0) {
+        atomicAdd(d.nstats + 0, c_pass);
+        atomicAdd(d.nstats + 1, c_eval);
+        atomicAdd(d.nstats + 2, c_nr);
+        atomicAdd(d.nstats + 3, c_tau);
+        atomicAdd(d.nstats + 4, c_vox);
+        atomicAdd(d.nstats + 5, c_npass);
+    }
     double acc[14];
 #pragma unroll
     for (int c = 0; c < 14; c++) acc[c] = lane < 5 ? accw[lane * 14 + c] : 0.0;

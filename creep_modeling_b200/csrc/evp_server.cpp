@@ -32,6 +32,7 @@ struct Request {
     unsigned long long id = 0;
     std::string fft, out;
     int mix = 1, modal = 0, precision = 0, flags = EVP_WRITE_FILES;
+    double deadline_s = 0.0;  // wall-clock budget from admission (0: none)
     int n1 = 0, n2 = 0, n3 = 0;
     unsigned long long foot = 0;
     int state = 0, status = 0, macrosteps = 0;
@@ -97,6 +98,7 @@ struct evp_server {
         if (rc != 0) {
             err = evp_last_error();
         } else {
+            if (r.deadline_s > 0.0) evp_set_deadline(h, r.deadline_s - secs(r.t_start, Clock::now()));
             int done = 0;
             while (true) {
                 rc = evp_advance(h, 1, &done);
@@ -218,6 +220,11 @@ int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const
 
 int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision, int flags,
                unsigned long long* ticket) {
+    return evp_submit_deadline(srv, fft_in, out_dir, mix, modal, precision, flags, 0.0, ticket);
+}
+
+int evp_submit_deadline(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision,
+                        int flags, double deadline_s, unsigned long long* ticket) {
     if (!srv || !fft_in || !ticket) return srv_fail("evp_submit: null argument", -7);
     if (precision != 0 && precision != 1) return srv_fail("evp_submit: precision must be 0 (plain FP64) or 1 (mixed)", -7);
     if ((flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) == 0) return srv_fail("evp_submit: flags must ask for EVP_WRITE_FILES or EVP_WRITE_CSV", -7);
@@ -228,6 +235,7 @@ int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix
     r.modal = modal;
     r.precision = precision;
     r.flags = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV | EVP_VERBOSE)) | (precision == 1 ? EVP_MIXED : 0);
+    r.deadline_s = deadline_s > 0.0 ? deadline_s : 0.0;
     if (!deck_grid(r.fft, r.n1, r.n2, r.n3)) return srv_fail("evp_submit: cannot read the grid size from " + r.fft, -1);
     r.foot = footprint(r.n1, r.n2, r.n3);
     r.t_submit = Clock::now();

@@ -15,6 +15,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <filesystem>
+#include <map>
 #include <mutex>
 #include <set>
 #include <cstdio>
@@ -122,6 +124,13 @@ public:
     std::vector<double> snap_dsim, snap_scau;
     bool has_thermo = false;
     std::vector<double> eth_soa;  // host staging of the thermal eigenstrain upload (kept until the copy completes)
+    // optional wall-clock budget: the solve ends with -8 at the first equilibrium iteration after it
+    bool has_deadline = false;
+    std::chrono::steady_clock::time_point deadline{};
+    void check_deadline() const {
+        if (has_deadline && std::chrono::steady_clock::now() > deadline)
+            throw SolveError("deadline exceeded: the solve's wall-clock budget ran out", -8);
+    }
 
     ProcessData& P() { return dk.process[ipr - 1]; }
 
@@ -129,7 +138,8 @@ public:
     T* dalloc(size_t n) {
         void* p = nullptr;
         if (n == 0) return nullptr;
-        CK(cudaMallocAsync(&p, n * sizeof(T), st));  // stream-ordered: no device-wide sync, so concurrent solves do not stall
+        // stream-ordered from the library's own pool: no device-wide sync, so concurrent solves do not stall
+        CK(cudaMallocFromPoolAsync(&p, n * sizeof(T), solver_pool(), st));
         allocs.push_back(p);
         return (T*)p;
     }
@@ -170,8 +180,10 @@ public:
         CK(cudaEventCreate(&e));
         return e;
     }
+    long long launches = 0;  // kernels launched by this solve (K() wrappers; k_grid_fft counts its five passes)
     template <class F>
-    void K(const char* name, F&& f) {
+    void K(const char* name, F&& f, int nlaunch = 1) {
+        launches += nlaunch;
         if (!profile) { f(); return; }
         int k = -1;
         for (size_t i = 0; i < ktimes.size(); i++)
@@ -209,21 +221,31 @@ public:
         if (*h_err & 4) throw SolveError("form_G failed (singular acoustic tensor or complex D operator)", -3);
     }
 
-    // The solver allocates stream-ordered from the device's default memory pool.  By default
-    // that pool hands freed memory back to the driver at every synchronisation, so each new
-    // solve would map its ~5 kB per voxel afresh; keeping it in the pool makes back-to-back
-    // and concurrent solves reuse it (the memory stays with this process until it exits).
-    static void keep_pool_memory() {
+    // The solver allocates stream-ordered from a memory pool of its own, one per device, that
+    // keeps freed memory instead of handing it back to the driver at every synchronisation:
+    // back-to-back and concurrent solves then reuse it rather than mapping ~2 kB per voxel
+    // afresh.  The device's default pool, which the embedding application (PyTorch's
+    // cudaMallocAsync backend, say) may use, is left as it is.  The pool's memory stays
+    // with this process until it exits.
+    static cudaMemPool_t solver_pool() {
         int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess) return;
+        if (cudaGetDevice(&dev) != cudaSuccess) throw SolveError("cudaGetDevice failed", -6);
         static std::mutex m;
-        static std::set<int> done;
+        static std::map<int, cudaMemPool_t> pools;
         std::lock_guard<std::mutex> lk(m);
-        if (!done.insert(dev).second) return;
+        auto it = pools.find(dev);
+        if (it != pools.end()) return it->second;
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
         cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+        CK(cudaMemPoolCreate(&pool, &props));
         unsigned long long keep = ~0ull;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools.emplace(dev, pool);
+        return pool;
     }
 
     // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
@@ -236,9 +258,14 @@ public:
         outdir = out.empty() ? std::string("evpfft_outputs/") : out;
         if (write_files) {
             mkdir_p(outdir);
-            // old *.vtk / *.out are removed at start (LS-EVPFFT.f90:145-146)
-            std::string cmd = "find \"" + outdir + "\" -maxdepth 1 -type f \\( -name '*.vtk' -o -name '*.out' \\) -delete 2>/dev/null";
-            if (std::system(cmd.c_str()) != 0) {}
+            // old *.vtk / *.out are removed at start (LS-EVPFFT.f90:145-146): regular files directly
+            // in the output directory, no shell involved
+            std::error_code ec;
+            for (const auto& e : std::filesystem::directory_iterator(outdir, ec)) {
+                const std::string ext = e.path().extension().string();
+                std::error_code ec2;
+                if ((ext == ".vtk" || ext == ".out") && e.is_regular_file(ec2)) std::filesystem::remove(e.path(), ec2);
+            }
         }
         try {
             dk = parse_deck(fft_in);
@@ -252,7 +279,6 @@ public:
         CK(cudaEventCreate(&ev1));
         static std::once_flag configured;
         std::call_once(configured, [] { fft_configure(); });
-        keep_pool_memory();
         allocate();
         upload_and_init();
         modal = (modal_flag != 0);
@@ -322,6 +348,8 @@ public:
         d.red = dalloc<double>(RED_OUT_SIZE);
         d.counters = dalloc<unsigned int>(CNT_N);
         d.err = dalloc<int>(1);
+        d.nstats = profile ? dalloc<unsigned long long>(8) : nullptr;
+        if (d.nstats) CK(cudaMemsetAsync(d.nstats, 0, 8 * sizeof(unsigned long long), st));
         CK(cudaMemsetAsync(d.counters, 0, CNT_N * sizeof(unsigned int), st));
         CK(cudaMemsetAsync(d.err, 0, sizeof(int), st));
         CK(cudaMemsetAsync(d.red, 0, RED_OUT_SIZE * sizeof(double), st));
@@ -470,7 +498,7 @@ public:
         fetch_red();
         // release the start-up staging buffers
         for (void* p : {(void*)d_eul, (void*)d_gr, (void*)d_hp}) {
-            cudaFree(p);
+            CK(cudaFreeAsync(p, st));
             allocs.erase(std::find(allocs.begin(), allocs.end(), p));
         }
     }
@@ -694,6 +722,7 @@ public:
                 prec_it = prec;
                 err_hist.clear();
             }
+            check_deadline();
             iter++;
             total_iters++;
             if (verbose) {
@@ -771,7 +800,7 @@ public:
                 launch_fft_y(d, pl2, 3, true, st);
                 XinvParams xp{};
                 launch_fft_x_inv(d, pl1, 1, xp, st);
-            });
+            }, 5);
             K("k_cell2node", [&] { launch_cell2node(d, p.tdot, p.igamma, st); });
         }
         Upd1Params u1;
@@ -797,7 +826,10 @@ public:
         evmavg = evmavg + dvmavg * p.tdot;
         const double Lref = std::max(lvmavg, EVP_TINY);
         K("k_diag", [&] { launch_diag(d, std::max(1.0e-12 * Lref, EVP_TINY), st); });
-        // time bookkeeping and the tdot ramp are host-only; they fix the tdot calc_c0 sees
+        // time bookkeeping and the tdot ramp are host-only; they fix the tdot calc_c0 sees.  The
+        // VTK "last step" test below uses the step count from before the ramp, as the reference
+        // writes its fields before ramping (LS-EVPFFT.f90:525-535, then 557-581).
+        const int nsteps_written = p.nsteps;
         const double tdot_used = p.tdot;
         const double tdotref_used = p.tdotref;
         if (p.ictrl == -1) {
@@ -864,7 +896,7 @@ public:
         dvmpavg = vm_strain(edotpavg);
         if (p.iwfields == 1) {
             const int aw = std::abs(p.iwstep);
-            const bool due = (aw != 0 && imicro % aw == 0) || (p.iwstep < 0 && imicro == p.nsteps);
+            const bool due = (aw != 0 && imicro % aw == 0) || (p.iwstep < 0 && imicro == nsteps_written);
             if (due && write_vtk_files) write_vtk(imacroloop);
         }
         finish_diag();
@@ -1300,6 +1332,30 @@ int evp_kernel_times(evp_solve* h, char* names, long long* launches, double* ms,
         n++;
     }
     return n;
+}
+
+int evp_set_deadline(evp_solve* h, double seconds) {
+    if (!h) return fail("evp_set_deadline: null handle", -7);
+    h->s.has_deadline = seconds > 0.0;
+    h->s.deadline = std::chrono::steady_clock::now() +
+                    std::chrono::duration_cast<std::chrono::steady_clock::duration>(std::chrono::duration<double>(seconds > 0.0 ? seconds : 0.0));
+    return 0;
+}
+
+long long evp_kernel_launches(evp_solve* h) { return h ? h->s.launches : -1; }
+
+int evp_newton_stats(evp_solve* h, long long* out6) {
+    if (!h || !out6) return fail("evp_newton_stats: null argument", -7);
+    if (!h->s.d.nstats) return fail("evp_newton_stats: the solve was not opened with EVP_PROFILE", -7);
+    unsigned long long v[8];
+    try {
+        CK(cudaMemcpyAsync(v, h->s.d.nstats, sizeof(v), cudaMemcpyDeviceToHost, h->s.st));
+        h->s.sync();
+    } catch (SolveError& e) {
+        return fail(e.what(), e.code);
+    }
+    for (int i = 0; i < 6; i++) out6[i] = (long long)v[i];
+    return 0;
 }
 
 int evp_close(evp_solve* h) {

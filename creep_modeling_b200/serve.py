@@ -11,15 +11,17 @@ writing the same files as the executable.
 ``python -m creep_modeling_b200.serve --socket PATH`` hosts a server behind a
 local Unix socket.  With ``EVP_SERVER_SOCKET=PATH`` in its environment the
 ``LS-EVPFFT`` shim submits its solve there and blocks until the files are
-written, so concurrent shim processes (calibrate.py's) share one GPU.  The
-socket has no authentication: any local user who can open it can submit decks,
-so create it in a directory only the intended users can reach.
+written, so concurrent shim processes (calibrate.py's) share one GPU.  Requests
+and answers are JSON (never pickled objects), every request field is checked,
+and the socket file is created with mode 0600: only its owner can connect.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes
+import json
 import os
+import socket
 import threading
 from pathlib import Path
 
@@ -49,13 +51,15 @@ class Server:
         self._h = h
         self._lock = threading.Lock()
 
-    def submit(self, fft_in, out_dir, mix: int = 1, modal: int = 0, precision: int = 0, csv_only: bool = False) -> int:
-        """Queue one solve; returns its ticket.  csv_only: results/diagnostics without VTK."""
+    def submit(self, fft_in, out_dir, mix: int = 1, modal: int = 0, precision: int = 0, csv_only: bool = False,
+               deadline_s: float | None = None) -> int:
+        """Queue one solve; returns its ticket.  csv_only: results/diagnostics without VTK.
+        deadline_s: wall-clock budget from admission; an overrunning solve ends with status -8."""
         L = _lib.load()
         t = ctypes.c_ulonglong()
         flags = 4 if csv_only else 1  # EVP_WRITE_CSV / EVP_WRITE_FILES
-        _lib.check(L.evp_submit(self._h, str(fft_in).encode(), str(out_dir).encode(), int(mix), int(modal),
-                                int(precision), flags, ctypes.byref(t)))
+        _lib.check(L.evp_submit_deadline(self._h, str(fft_in).encode(), str(out_dir).encode(), int(mix), int(modal),
+                                         int(precision), flags, float(deadline_s or 0.0), ctypes.byref(t)))
         return int(t.value)
 
     def poll(self, ticket: int) -> dict:
@@ -85,34 +89,89 @@ class Server:
 
 
 # ---------------------------------------------------------------- local socket front end
+# Wire format: one JSON object per connection in each direction, terminated by a
+# newline.  JSON carries only data (no pickled objects), requests are checked
+# field by field, and the socket file is created with mode 0600 so only its
+# owner can connect.
+MAX_REQUEST_BYTES = 64 * 1024
+_FIELDS = {"in": str, "out": str, "mix": int, "modal": int, "precision": int, "csv_only": bool}
+
+
+def _read_line(sock, limit: int = MAX_REQUEST_BYTES) -> bytes:
+    buf = bytearray()
+    while b"\n" not in buf:
+        chunk = sock.recv(4096)
+        if not chunk:
+            break
+        buf += chunk
+        if len(buf) > limit:
+            raise ValueError(f"request longer than {limit} bytes")
+    return bytes(buf.split(b"\n", 1)[0])
+
+
+def parse_request(raw: bytes) -> dict:
+    """Decode and check one request: {"in": str, "out": str} plus optional mix, modal,
+    precision (ints) and csv_only (bool).  Raises ValueError on anything else."""
+    try:
+        req = json.loads(raw.decode("utf-8"))
+    except (UnicodeDecodeError, json.JSONDecodeError) as e:
+        raise ValueError(f"not a JSON object: {e}") from None
+    if not isinstance(req, dict):
+        raise ValueError("request must be a JSON object")
+    extra = set(req) - set(_FIELDS)
+    if extra:
+        raise ValueError(f"unknown fields {sorted(extra)}")
+    for key in ("in", "out"):
+        if key not in req:
+            raise ValueError(f"missing field {key!r}")
+    out = {"mix": 1, "modal": 0, "precision": 0, "csv_only": False}
+    for key, typ in _FIELDS.items():
+        if key not in req:
+            continue
+        v = req[key]
+        ok = isinstance(v, typ) and not (typ is int and isinstance(v, bool))
+        if not ok or (typ is str and (not v or "\0" in v)):
+            raise ValueError(f"field {key!r} must be a {typ.__name__}")
+        out[key] = v
+    return out
+
+
 def serve_socket(path: str, backend, stop: threading.Event | None = None) -> None:
     """Accept requests on a Unix socket and answer each with its final status.
 
-    A request is a dict {"in", "out", "mix", "modal", "precision", "csv_only"};
-    the answer is the status dict of :meth:`Server.wait`, or {"status": -7,
-    "error": ...} for a malformed request.  ``backend`` is a :class:`Server`
-    (anything with its submit/wait methods).  Each connection is served on its
-    own thread, so a client blocks only on its own solve."""
-    from multiprocessing.connection import Listener
-
+    A request is the JSON object {"in", "out", "mix", "modal", "precision",
+    "csv_only"}; the answer is the status dict of :meth:`Server.wait`, or
+    {"status": -7, "error": ...} for a malformed request.  ``backend`` is a
+    :class:`Server` (anything with its submit/wait methods).  Each connection is
+    served on its own thread, so a client blocks only on its own solve."""
     if os.path.exists(path):
         os.unlink(path)
-    listener = Listener(path, family="AF_UNIX")
+    lsock = socket.socket(socket.AF_UNIX, socket.SOCK_STREAM)
+    old = os.umask(0o177)  # the socket file is created owner read/write only
+    try:
+        lsock.bind(path)
+    finally:
+        os.umask(old)
+    os.chmod(path, 0o600)
+    lsock.listen(64)
+
+    def answer(conn, obj):
+        conn.sendall(json.dumps(obj).encode() + b"\n")
 
     def handle(conn):
         try:
-            req = conn.recv()
             try:
-                t = backend.submit(req["in"], req["out"], int(req.get("mix", 1)), int(req.get("modal", 0)),
-                                   int(req.get("precision", 0)), bool(req.get("csv_only", False)))
+                req = parse_request(_read_line(conn))
+            except ValueError as e:
+                answer(conn, {"state": "done", "status": -7, "error": f"bad request: {e}"})
+                return
+            try:
+                t = backend.submit(req["in"], req["out"], req["mix"], req["modal"], req["precision"], req["csv_only"])
             except _lib.EvpError as e:
-                conn.send({"state": "done", "status": e.code, "error": str(e)})
+                answer(conn, {"state": "done", "status": e.code, "error": str(e)})
                 return
-            except (KeyError, TypeError, ValueError) as e:
-                conn.send({"state": "done", "status": -7, "error": f"bad request: {e}"})
-                return
-            conn.send(backend.wait(t))
-        except EOFError:
+            answer(conn, backend.wait(t))
+        except OSError:
             pass
         finally:
             conn.close()
@@ -120,23 +179,24 @@ def serve_socket(path: str, backend, stop: threading.Event | None = None) -> Non
     try:
         while stop is None or not stop.is_set():
             try:
-                conn = listener.accept()
+                conn, _ = lsock.accept()
             except OSError:
                 break
             threading.Thread(target=handle, args=(conn,), daemon=True).start()
     finally:
-        listener.close()
+        lsock.close()
 
 
 def submit_via_socket(path: str, fft_in, out_dir, mix: int = 1, modal: int = 0, precision: int = 0,
                       csv_only: bool = False) -> dict:
     """Send one request to a socket server and wait for its final status."""
-    from multiprocessing.connection import Client
-
-    with Client(path, family="AF_UNIX") as c:
-        c.send({"in": str(fft_in), "out": str(out_dir), "mix": int(mix), "modal": int(modal), "precision": int(precision),
-                "csv_only": bool(csv_only)})
-        return c.recv()
+    with socket.socket(socket.AF_UNIX, socket.SOCK_STREAM) as c:
+        c.connect(path)
+        req = {"in": str(fft_in), "out": str(out_dir), "mix": int(mix), "modal": int(modal), "precision": int(precision),
+               "csv_only": bool(csv_only)}
+        c.sendall(json.dumps(req).encode() + b"\n")
+        raw = _read_line(c, 1 << 20)
+    return json.loads(raw.decode()) if raw else {"state": "done", "status": -7, "error": "server closed the connection"}
 
 
 def main(argv=None) -> int:

@@ -102,6 +102,17 @@ class Solve:
             out[nm] = (int(launches[i]), float(ms[i]))
         return out
 
+    def launches(self) -> int:
+        """Kernels launched by this solve so far."""
+        return int(_lib.load().evp_kernel_launches(self._h))
+
+    def newton_stats(self) -> dict:
+        """Activity counters of the local Newton kernel (profiled solves only)."""
+        v = (ctypes.c_longlong * 6)()
+        _lib.check(_lib.load().evp_newton_stats(self._h, v))
+        keys = ("eval_passes", "evaluations", "newton_steps", "hardening_updates", "voxels", "newton_passes")
+        return dict(zip(keys, (int(x) for x in v)))
+
     def stats(self) -> _lib.Report:
         rep = _lib.Report()
         _lib.check(_lib.load().evp_stats(self._h, ctypes.byref(rep)))

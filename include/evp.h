@@ -13,7 +13,8 @@
  * Status codes: 0 ok; -1 deck or input-file error; -2 deck feature not
  * supported by this build; -3 singular matrix (the reference's `stop 1` in
  * lu_inverse / lu_eqsystem / dgesvd); -4 non-convergence or non-finite
- * state; -5 output-file error; -6 CUDA error or no device; -7 bad argument.
+ * state; -5 output-file error; -6 CUDA error or no device; -7 bad argument;
+ * -8 the solve's wall-clock deadline passed (evp_set_deadline, evp_submit_deadline).
  */
 #ifndef EVP_B200_H
 #define EVP_B200_H
@@ -70,12 +71,25 @@ int evp_get_field(evp_solve* s, const char* name, double* host_out, long long ca
  * diagnostics.csv row (44 values, types.f90:787-798 order). */
 int evp_last_rows(evp_solve* s, double* results51, double* diag44);
 int evp_stats(evp_solve* s, evp_report* out);
+/* Wall-clock budget for the rest of the solve, in seconds from now (<= 0: none).  The
+ * solve checks it before every equilibrium iteration and, once it has passed, ends
+ * with -8; the files written so far stay.  The reference has no counterpart (its
+ * callers can only kill the process). */
+int evp_set_deadline(evp_solve* s, double seconds);
 int evp_close(evp_solve* s);
 
 /* Per-kernel device time under EVP_PROFILE: fills up to cap entries of
  * names (each a NUL-terminated string of at most 31 chars, stored in
  * names[32*i]), launches and milliseconds; returns the number of kernels. */
 int evp_kernel_times(evp_solve* s, char* names, long long* launches, double* ms, int cap);
+/* Number of kernels this solve has launched so far (with or without EVP_PROFILE); -1 for a null handle. */
+long long evp_kernel_launches(evp_solve* s);
+/* Activity counters of the local Newton kernel since open (EVP_PROFILE solves only; no
+ * counterpart in the reference): out6[0] warp passes of the evaluation loop, [1] voxel
+ * evaluations done in those passes (five voxel groups per warp), [2] Newton steps, [3]
+ * hardening updates, [4] voxels solved, [5] warp passes of the Newton-step loop.
+ * [1] / (5 [0]) is the fraction of voxel slots that did useful work. */
+int evp_newton_stats(evp_solve* s, long long* out6);
 
 /* Operator-level entry: applies the periodic Green operator of a homogeneous
  * reference medium to a polarization field, the inner operator of every
@@ -143,6 +157,11 @@ int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const
  * EVP_WRITE_CSV (results and diagnostics only).  The ticket identifies it. */
 int evp_submit(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision, int flags,
                unsigned long long* ticket);
+/* evp_submit with a wall-clock budget: deadline_s seconds from the solve's admission
+ * (<= 0: none); a solve that overruns it ends between equilibrium iterations with
+ * status -8 while the other solves continue. */
+int evp_submit_deadline(evp_server* srv, const char* fft_in, const char* out_dir, int mix, int modal, int precision,
+                        int flags, double deadline_s, unsigned long long* ticket);
 /* Current state of a request (non-blocking). */
 int evp_poll(evp_server* srv, unsigned long long ticket, evp_status* st);
 /* Block until the request is done or timeout_s passes (timeout_s < 0: no limit);

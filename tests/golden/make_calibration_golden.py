@@ -6,10 +6,10 @@ Writes, next to this file:
 
 The reference's ``utils/`` package imports ``skopt`` (absent here) from
 ``config.py`` only for a search-space type that the loaders and metrics never
-use; a stub module satisfies that import.  Run in a checkout that has the
-reference next to it:
+use; a stub module satisfies that import.  The reference checkout is named by
+the first argument or by the EVP_REFERENCE environment variable:
 
-    python tests/golden/make_calibration_golden.py /root/reference
+    python tests/golden/make_calibration_golden.py PATH/TO/creep_modeling
 """
 import sys
 import types
@@ -70,4 +70,9 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EVP_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_calibration_golden.py PATH/TO/reference (or set EVP_REFERENCE)")
+    main(ref)

@@ -80,3 +80,35 @@ def test_budget_admits_one_at_a_time(tmp_path):
     assert sts[1]["queued_s"] >= 0.9 * sts[0]["run_s"]
     for i in range(len(ffts)):
         _same(tmp_path / f"alone{i}", tmp_path / f"one{i}")
+
+
+def test_failing_solves_are_isolated(tmp_path):
+    """Beside two good solves, one deck whose phase stiffness is singular (-3), one whose
+    microstructure file is missing (-1) and one that overruns its wall-clock budget (-8):
+    each failing request reports its own status and the good solves' files are the same
+    as when they run alone."""
+    good = _cases(tmp_path)[:2]
+    for i, f in enumerate(good):
+        _alone(f, tmp_path / f"alone{i}")
+    sing = decks.write_case(decks.case_c1(nsteps=2), tmp_path / "singular")
+    (sing.parent / "cuel.sx").write_text("0 \t\t\t\t\tISO\n" + "0.0 0.0 0.0 0.0 0.0 0.0\n" * 6)
+    missing = decks.write_case(decks.case_c1(nsteps=2), tmp_path / "missing")
+    (missing.parent / "micro.dat").unlink()
+    big = decks.case_c1(nsteps=100)
+    big.n = 32  # 100 increments at 32^3: seconds of work, far beyond its budget
+    slow = decks.write_case(big, tmp_path / "slow")
+    with Server(0, 8) as srv:
+        tg = [srv.submit(f, tmp_path / f"mix{i}", mix=1, modal=0, csv_only=True) for i, f in enumerate(good)]
+        ts = srv.submit(sing, tmp_path / "o_sing", mix=1, modal=0, csv_only=True)
+        tm = srv.submit(missing, tmp_path / "o_miss", mix=1, modal=0, csv_only=True)
+        td = srv.submit(slow, tmp_path / "o_slow", mix=1, modal=0, csv_only=True, deadline_s=0.3)
+        sts = [srv.wait(t, timeout=600) for t in tg]
+        s_sing, s_miss, s_slow = srv.wait(ts, timeout=600), srv.wait(tm, timeout=600), srv.wait(td, timeout=600)
+    assert all(st["status"] == 0 for st in sts), sts
+    assert s_sing["status"] == -3 and "ingular" in s_sing["error"], s_sing
+    assert s_miss["status"] == -1, s_miss
+    assert s_slow["status"] == -8 and "deadline" in s_slow["error"], s_slow
+    assert 0 < s_slow["macrosteps"] < 100
+    assert s_slow["run_s"] < 30.0
+    for i in range(len(good)):
+        _same(tmp_path / f"alone{i}", tmp_path / f"mix{i}")

@@ -103,3 +103,39 @@ def test_server_open_without_device():
     h = ctypes.c_void_p()
     assert L.evp_server_open(0, 4, None, ctypes.byref(h)) == -6
     assert b"CUDA" in L.evp_last_error()
+
+
+def test_socket_file_is_owner_only(fake_server):
+    import stat
+
+    path, _ = fake_server
+    assert stat.S_IMODE(os.stat(path).st_mode) == 0o600
+
+
+@pytest.mark.parametrize("raw", [
+    b"not json",
+    b"[1, 2]",
+    b'{"in": "a"}',
+    b'{"in": "a", "out": "b", "mix": "1"}',
+    b'{"in": "a", "out": "b", "mix": true}',
+    b'{"in": 3, "out": "b"}',
+    b'{"in": "a", "out": "b", "cmd": "x"}',
+    b'{"in": "", "out": "b"}',
+])
+def test_malformed_requests_are_refused(raw):
+    with pytest.raises(ValueError):
+        serve.parse_request(raw)
+
+
+def test_malformed_request_answered_with_status(fake_server):
+    import json
+    import socket as so
+
+    path, backend = fake_server
+    n0 = len(backend.requests)
+    with so.socket(so.AF_UNIX, so.SOCK_STREAM) as c:
+        c.connect(path)
+        c.sendall(b'{"in": "a", "out": "b", "precision": "1"}\n')
+        st = json.loads(serve._read_line(c).decode())
+    assert st["status"] == -7 and "precision" in st["error"]
+    assert len(backend.requests) == n0

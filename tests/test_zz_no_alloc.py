@@ -32,16 +32,21 @@ def _call(fn, tau_dev, out_dev, shape, c0, s0):
     return fn(ctypes.c_void_p(tau_dev.data_ptr()), ctypes.c_void_p(out_dev.data_ptr()), *shape, p(c0), p(s0), None)
 
 
-def test_noalloc_matches_allocating_entry_twice():
+# 32^3 (power-of-two passes), 24 x 20 x 12 (radix-3/5 stages, a non-cubic box), 8 x 8 x 1 (a 2-D grid)
+# and 30 x 32 x 34, a non-cubic grid at the scratch limit: (30/2 + 1) * 32 * 34 = 17408 half-spectrum points.
+SHAPES = [(32, 32, 32), (24, 20, 12), (8, 8, 1), (30, 32, 34)]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
+def test_noalloc_matches_allocating_entry_twice(shape):
     import torch
 
     from creep_modeling_b200 import _lib
 
     L = _lib.load()
     c0, s0 = _medium()
-    shape = (32, 32, 32)  # the largest grid the fixed scratch takes
     n = int(np.prod(shape))
-    rng = np.random.default_rng(11)
+    rng = np.random.default_rng(11 + n)
     for call in range(2):
         tau = torch.from_numpy(rng.standard_normal((9, n))).cuda()
         out_ref = torch.empty_like(tau)
