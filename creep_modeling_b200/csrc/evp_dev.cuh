@@ -47,6 +47,16 @@ enum : int {
 
 enum : int { CNT_SGAVG = 0, CNT_XINV, CNT_CORR, CNT_NEWTON, CNT_INIT, CNT_UPD1, CNT_UPD2, CNT_UPD3, CNT_DIAG, CNT_DIAG2, CNT_C0, CNT_KIN, CNT_G0, CNT_DISP, CNT_N };
 
+// Block coordinates of a kernel body: the hardware block index for a launch over one
+// solve, or the solve-local block index that a batched launch decodes from its job
+// table (nx: the solve-local grid extent along x, which is the whole grid of a 1-D launch).
+struct VB {
+    int x, y, z, nx;
+};
+#ifdef __CUDACC__
+__device__ __forceinline__ VB hw_vb() { return VB{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)gridDim.x}; }
+#endif
+
 struct FftPlan1D {
     int n;
     int nst;

@@ -235,7 +235,7 @@ __device__ __forceinline__ const float2* twid<float2>(const Dev& d, int axis) {
 // ---------------------------------------------------------------- x forward (R2C)
 // mode 0: P'_ij = J * ((sigma - <sigma>) F^{-T})_ij ; mode 1: (L F)_ij (grid update)
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, 2) k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
+__device__ __forceinline__ void body_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int G, int mode, int sg_off, const VB& vb) {
     using Re = typename CxT<CT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(256, 2) k_fft_x_fwd(Dev d, FftPlan1D pl, int G
     const long long N = d.N;
     const int nrows = d.n2 * d.n3;
     const int P = 9 * G;
-    const int pair0 = blockIdx.x * G;
+    const int pair0 = vb.x * G;
     __shared__ double sga[6];
     if (mode == 0 && threadIdx.x < 6) sga[threadIdx.x] = __ldcg(&d.red[sg_off + threadIdx.x]);
     __syncthreads();
@@ -295,14 +295,18 @@ __global__ void __launch_bounds__(256, 2) k_fft_x_fwd(Dev d, FftPlan1D pl, int G
         if (ra + 1 < nrows) spec[((long long)c * nrows + ra + 1) * n1h + k] = Xb;
     }
 }
+template <int RS, class CT>
+__global__ void __launch_bounds__(256, 2) k_fft_x_fwd(Dev d, FftPlan1D pl, int G, int mode, int sg_off) {
+    body_fft_x_fwd<RS, CT>(d, pl, G, mode, sg_off, hw_vb());
+}
 
 // ---------------------------------------------------------------- y (C2C)
 template <bool INV, int RS, class CT>
-__global__ void __launch_bounds__(256, 2) k_fft_y(Dev d, FftPlan1D pl, int T) {
+__device__ __forceinline__ void body_fft_y(const Dev& d, const FftPlan1D& pl, int T, const VB& vb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
     const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
-    const int kx0 = blockIdx.x * T, k3 = blockIdx.y, c = blockIdx.z;
+    const int kx0 = vb.x * T, k3 = vb.y, c = vb.z;
     CT* base = reinterpret_cast<CT*>(d.spec) + ((long long)c * n3 + k3) * n2 * n1h;
     for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
         const int t = idx % T, j = idx / T, kx = kx0 + t;
@@ -315,6 +319,8 @@ __global__ void __launch_bounds__(256, 2) k_fft_y(Dev d, FftPlan1D pl, int T) {
         if (kx < n1h) base[(long long)j * n1h + kx] = s[j * T + t];
     }
 }
+template <bool INV, int RS, class CT>
+__global__ void __launch_bounds__(256, 2) k_fft_y(Dev d, FftPlan1D pl, int T) { body_fft_y<INV, RS, CT>(d, pl, T, hw_vb()); }
 
 // ---------------------------------------------------------------- z fused with the Green operator
 __device__ __forceinline__ double xi_of(int k, int n) {
@@ -343,14 +349,15 @@ __device__ __forceinline__ int inv3_any(const float* a, float* ai) {
 }
 
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, 2) k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g, const double* __restrict__ s0g) {
+__device__ __forceinline__ void body_fft_z_green(const Dev& d, const FftPlan1D& pl, int T, const double* __restrict__ c0g,
+                                                 const double* __restrict__ s0g, const VB& vb) {
     using Re = typename CxT<CT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
     CT* const spec = reinterpret_cast<CT*>(d.spec);
     __shared__ Re c0[81], s0[81];
     const int n1 = d.n1, n2 = d.n2, n3 = d.n3, n1h = d.n1h;
-    const int kx0 = blockIdx.x * T, j = blockIdx.y;
+    const int kx0 = vb.x * T, j = vb.y;
     const int P = 9 * T;
     for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = (Re)c0g[i]; s0[i] = (Re)s0g[i]; }
     const long long plane = (long long)n2 * n1h;
@@ -444,6 +451,11 @@ __global__ void __launch_bounds__(256, 2) k_fft_z_green(Dev d, FftPlan1D pl, int
         const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
         if (kx < n1h) spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] = s[k3 * P + c * T + t];
     }
+}
+template <int RS, class CT>
+__global__ void __launch_bounds__(256, 2) k_fft_z_green(Dev d, FftPlan1D pl, int T, const double* __restrict__ c0g,
+                                                        const double* __restrict__ s0g) {
+    body_fft_z_green<RS, CT>(d, pl, T, c0g, s0g, hw_vb());
 }
 
 // ---------------------------------------------------------------- z fused with the spectral integration (grid update)
@@ -567,7 +579,8 @@ __global__ void __launch_bounds__(256, 2) k_fft_z_grad(Dev d, FftPlan1D pl, int 
 
 // ---------------------------------------------------------------- x inverse (C2R)
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, 2) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
+__device__ __forceinline__ void body_fft_x_inv(const Dev& d, const FftPlan1D& pl, int G, int ncomp, int mode, const XinvParams& xp,
+                                               const VB& vb) {
     using Re = typename CxT<CT>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* const s = reinterpret_cast<CT*>(smem_raw);
@@ -576,7 +589,7 @@ __global__ void __launch_bounds__(256, 2) k_fft_x_inv(Dev d, FftPlan1D pl, int G
     const long long N = d.N;
     const int nrows = d.n2 * d.n3;
     const int P = ncomp * G;
-    const int pair0 = blockIdx.x * G;
+    const int pair0 = vb.x * G;
     const bool even = (n1 % 2 == 0);
     for (int idx = threadIdx.x; idx < P * n1; idx += blockDim.x) {
         const int x = idx % n1, p = idx / n1;
@@ -636,19 +649,19 @@ __global__ void __launch_bounds__(256, 2) k_fft_x_inv(Dev d, FftPlan1D pl, int G
         for (int f = 0; f < 9; f++) {
             double x = lane < nw ? sh[f][lane] : 0.0;
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) d.partials[(size_t)f * gridDim.x + blockIdx.x] = x;
+            if (lane == 0) d.partials[(size_t)f * vb.nx + vb.x] = x;
         }
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(d.counters + CNT_XINV, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) last = (atomicAdd(d.counters + CNT_XINV, 1u) == (unsigned)vb.nx - 1u);
     __syncthreads();
     __shared__ double fsum[9];
     if (last) {  // fold the block partials: one warp per field, fixed order
         __threadfence();
         for (int f = warp; f < 9; f += nw) {
             double x = 0.0;
-            for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(&d.partials[(size_t)f * gridDim.x + b]);
+            for (int b = lane; b < vb.nx; b += 32) x += __ldcg(&d.partials[(size_t)f * vb.nx + b]);
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
             if (lane == 0) fsum[f] = x;
         }
@@ -664,6 +677,10 @@ __global__ void __launch_bounds__(256, 2) k_fft_x_inv(Dev d, FftPlan1D pl, int G
         for (int f = 0; f < 9; f++) d.red[OFF_DU + f] = du[f];
         d.counters[CNT_XINV] = 0;
     }
+}
+template <int RS, class CT>
+__global__ void __launch_bounds__(256, 2) k_fft_x_inv(Dev d, FftPlan1D pl, int G, int ncomp, int mode, XinvParams xp) {
+    body_fft_x_inv<RS, CT>(d, pl, G, ncomp, mode, xp, hw_vb());
 }
 
 // ---------------------------------------------------------------- standalone Green-operator application

@@ -34,7 +34,7 @@ constexpr int kC0Block = 64;
 
 // ---------------------------------------------------------------- reductions
 // NS sums then NM maxima per thread -> one partial per block (stored field-major,
-// partials[f * gridDim.x + block]) -> the last block to finish folds them: one
+// partials[f * nblocks + block], in the body's block coordinates) -> the last block to finish folds them: one
 // warp per field, lane l adding blocks l, l + 32, ... in order, then a fixed
 // shuffle tree, so the result does not depend on timing.
 __device__ __forceinline__ double fold_sum(const double* partials, int nblk, int f, int lane) {
@@ -53,7 +53,8 @@ __device__ __forceinline__ double fold_max(const double* partials, int nblk, int
 }
 
 template <int NS, int NM>
-__device__ void reduce_store(const double* sums, const double* maxs, double* partials, double* out, unsigned int* counter) {
+__device__ void reduce_store(const double* sums, const double* maxs, double* partials, double* out, unsigned int* counter,
+                             const VB& vb) {
     constexpr int NF = NS + NM;
     __shared__ double sh[NF][32];
     __shared__ bool last;
@@ -77,17 +78,17 @@ __device__ void reduce_store(const double* sums, const double* maxs, double* par
                 double y = __shfl_down_sync(0xffffffffu, x, o);
                 x = (f < NS) ? x + y : fmax(x, y);
             }
-            if (lane == 0) partials[(size_t)f * gridDim.x + blockIdx.x] = x;
+            if (lane == 0) partials[(size_t)f * vb.nx + vb.x] = x;
         }
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == (unsigned)vb.nx - 1u);
     __syncthreads();
     if (last) {
         __threadfence();
         for (int f = warp; f < NF; f += nw) {
-            const double x = (f < NS) ? fold_sum(partials, gridDim.x, f, lane) : fold_max(partials, gridDim.x, f, lane);
+            const double x = (f < NS) ? fold_sum(partials, vb.nx, f, lane) : fold_max(partials, vb.nx, f, lane);
             if (lane == 0) out[f] = x;
         }
         if (threadIdx.x == 0) *counter = 0;
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(kBlock) k_init(Dev d, const double* __restrict
             d.trialtau[(2 * s + 1) * N + v] = c2;
         }
     }
-    reduce_store<36, 0>(sums, nullptr, d.partials, d.red + OFF_INIT, d.counters + CNT_INIT);
+    reduce_store<36, 0>(sums, nullptr, d.partials, d.red + OFF_INIT, d.counters + CNT_INIT, hw_vb());
 }
 
 void launch_init(const Dev& d, const double* euler, const int* grain, const double* hp, const double* udot9, const double* u6t,
@@ -257,23 +258,24 @@ __global__ void __launch_bounds__(kBlock) k_dispini(Dev d, const double* __restr
         sums[28] += gas ? d.wgt * J : 0.0;
         sums[29] += J * d.wgt;
     }
-    reduce_store<30, 0>(sums, nullptr, d.partials, d.red + OFF_DISP, d.counters + CNT_DISP);
+    reduce_store<30, 0>(sums, nullptr, d.partials, d.red + OFF_DISP, d.counters + CNT_DISP, hw_vb());
 }
 void launch_dispini(const Dev& d, const double* grad, double delt, cudaStream_t st) {
     k_dispini<<<d.grid, kBlock, 0, st>>>(d, grad, delt);
 }
 
 // ---------------------------------------------------------------- k_sgavg
-__global__ void __launch_bounds__(kBlock) k_sgavg(Dev d) {
+__device__ __forceinline__ void body_sgavg(const Dev& d, const VB& vb) {
     const long long N = d.N;
     double s[6] = {0, 0, 0, 0, 0, 0};
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+    for (long long v = vb.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)vb.nx * blockDim.x) {
         double w = d.wgtc[v];
 #pragma unroll
         for (int c = 0; c < 6; c++) s[c] += d.sg[c * N + v] * w;
     }
-    reduce_store<6, 0>(s, nullptr, d.partials, d.red + OFF_SGAVG, d.counters + CNT_SGAVG);
+    reduce_store<6, 0>(s, nullptr, d.partials, d.red + OFF_SGAVG, d.counters + CNT_SGAVG, vb);
 }
+__global__ void __launch_bounds__(kBlock) k_sgavg(Dev d) { body_sgavg(d, hw_vb()); }
 void launch_sgavg(const Dev& d, cudaStream_t st) { k_sgavg<<<d.grid, kBlock, 0, st>>>(d); }
 
 // ---------------------------------------------------------------- b-basis congruence
@@ -427,7 +429,7 @@ void launch_gas_compl(const Dev& d, double tdot, double complgas, int modal, cud
 
 // ---------------------------------------------------------------- k_corr
 // velgrad += (dvelgradref + du) F^{-1}; averages; dL statistics; mixing.
-__global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) {
+__device__ __forceinline__ void body_corr(const Dev& d, const CorrParams& p, const VB& vb) {
     const long long N = d.N;
     __shared__ double du[9];
     if (threadIdx.x < 9) du[threadIdx.x] = __ldcg(&d.red[OFF_DU + threadIdx.x]);
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) {
     double s[31];
 #pragma unroll
     for (int c = 0; c < 31; c++) s[c] = 0.0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+    for (long long v = vb.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)vb.nx * blockDim.x) {
         double t[9], fi[9], u[9], vg[9], vo[9];
         ld9(d.dvr, N, v, t);
         ld9(d.Finv, N, v, fi);
@@ -467,8 +469,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) {
         st9(d.velgrad, N, v, vg);
         st9(d.velgradold, N, v, vg);
     }
-    reduce_store<31, 0>(s, nullptr, d.partials, d.red + OFF_CORR, d.counters + CNT_CORR);
+    reduce_store<31, 0>(s, nullptr, d.partials, d.red + OFF_CORR, d.counters + CNT_CORR, vb);
 }
+__global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) { body_corr(d, p, hw_vb()); }
 // fewer blocks than the other voxel kernels: each thread handles several voxels, which spreads the
 // 31-field block reduction over more loads
 void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st) {
@@ -757,7 +760,7 @@ __global__ void __launch_bounds__(kNewtonBlock, 2) k_newton(Dev d, NewtonParams 
             s[8 + c] += s6v[c] * w;
         }
     }
-    reduce_store<14, 0>(s, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
+    reduce_store<14, 0>(s, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON, hw_vb());
 }
 // ---------------------------------------------------------------- k_newton6: six lanes per voxel
 // The local solve of k_newton with the voxel's operators held in registers for
@@ -811,7 +814,7 @@ __host__ __device__ constexpr size_t newton6_smem_bytes(int spl) {
 }
 
 template <int SPL, bool MODAL>
-__global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
+__device__ __forceinline__ void body_newton6(const Dev& d, const NewtonParams& p, const VB& vb) {
     constexpr bool kSm = newton6_cols_in_smem(SPL);
     extern __shared__ double dyn_smem[];
     double* const col = dyn_smem + (threadIdx.x >> 5) * newton6_col_rows(SPL) * kXStride + (threadIdx.x & 31);
@@ -830,8 +833,8 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
     double acc[14];
 #pragma unroll
     for (int c = 0; c < 14; c++) acc[c] = 0.0;
-    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long wid = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)vb.nx * blockDim.x) >> 5;
     const double tolt = fmax(p.error, p.erroral);
     for (long long v0 = wid * 5; v0 < N; v0 += nwarp * 5) {  // warp-uniform
         const bool valid = grp < 5 && v0 + grp < N;
@@ -1201,7 +1204,7 @@ __global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) {
             }
         }
     }
-    reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
+    reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON, vb);
 }
 
 // ---------------------------------------------------------------- shared-memory exchange of k_newton6p
@@ -1232,6 +1235,9 @@ __device__ __forceinline__ void xgather(const Xw& X, double x, double (&out)[6])
 #pragma unroll
     for (int c = 0; c < 6; c++) out[c] = row[X.base + c];
 }
+
+template <int SPL, bool MODAL>
+__global__ void __launch_bounds__(256, 2) k_newton6(Dev d, NewtonParams p) { body_newton6<SPL, MODAL>(d, p, hw_vb()); }
 
 // What the local solve reads of a phase, staged in shared memory once per block
 // (MS systems at most: 12 or 24).
@@ -1285,7 +1291,7 @@ __host__ __device__ constexpr size_t newton6p_smem_bytes(int spl, int nph) {
 // operator rows and per-system state live in shared memory, which keeps the
 // kernel within 128 registers with few spills (16 warps per SM).
 template <int SPL>
-__global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
+__device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& p, const VB& vb) {
     constexpr int MS = 6 * SPL;
     constexpr bool kSm = newton6p_cols_in_smem(SPL);
     extern __shared__ double dyn_smem[];
@@ -1334,8 +1340,8 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     __syncwarp();
     double* const accg = accw + (grp < 5 ? grp : 0) * 14;
     const double tolt = fmax(p.error, p.erroral);
-    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long wid = ((long long)vb.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)vb.nx * blockDim.x) >> 5;
     const bool stats = d.nstats != nullptr;
     unsigned long long c_pass = 0, c_eval = 0, c_nr = 0, c_tau = 0, c_vox = 0, c_npass = 0;  // warp-uniform counts
     const unsigned lead = 0x01041041u;  // lanes 0, 6, 12, 18, 24: one per voxel group
@@ -1727,8 +1733,11 @@ __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) {
     double acc[14];
 #pragma unroll
     for (int c = 0; c < 14; c++) acc[c] = lane < 5 ? accw[lane * 14 + c] : 0.0;
-    reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON);
+    reduce_store<14, 0>(acc, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON, vb);
 }
+
+template <int SPL>
+__global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) { body_newton6p<SPL>(d, p, hw_vb()); }
 
 void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
     // EVP_NEWTON_ONE_THREAD=1 selects the one-thread-per-voxel kernel, kept for comparison
@@ -1851,7 +1860,7 @@ __global__ void __launch_bounds__(kBlock) k_upd1(Dev d, Upd1Params p) {
         else s[36] += d.wgt * detF;
         s[38] += detF * d.wgt;
     }
-    reduce_store<39, 1>(s, mx, d.partials, d.red + OFF_UPD1, d.counters + CNT_UPD1);
+    reduce_store<39, 1>(s, mx, d.partials, d.red + OFF_UPD1, d.counters + CNT_UPD1, hw_vb());
 }
 void launch_upd1(const Dev& d, const Upd1Params& p, cudaStream_t st) {
     if (d.nsys <= 12) k_upd1<12><<<d.grid, kBlock, 0, st>>>(d, p);
@@ -2057,7 +2066,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_upd3(Dev d, Upd3Params p) {
                 s[29] += fabs(gd[q]) * gs;
             }
     }
-    reduce_store<30, 0>(s, nullptr, d.partials, d.red + OFF_UPD3, d.counters + CNT_UPD3);
+    reduce_store<30, 0>(s, nullptr, d.partials, d.red + OFF_UPD3, d.counters + CNT_UPD3, hw_vb());
 }
 void launch_upd3(const Dev& d, const Upd3Params& p, cudaStream_t st) {
     if (d.nsys <= 12) k_upd3<12><<<d.grid, kBlock, 0, st>>>(d, p);
@@ -2141,7 +2150,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_diag(Dev d, double Lfloor) {
         pm[2 * blockIdx.x + 1] = b;
     }
     __syncthreads();
-    reduce_store<6, 13>(s, m, d.partials, d.red + OFF_DIAG, d.counters + CNT_DIAG);
+    reduce_store<6, 13>(s, m, d.partials, d.red + OFF_DIAG, d.counters + CNT_DIAG, hw_vb());
     // reduce_store reset the counter; use a second counter pass for the pairs
     __threadfence();
     __syncthreads();
@@ -2204,7 +2213,7 @@ __global__ void __launch_bounds__(kC0Block) k_c0(Dev d, double tdot, double tdot
 #pragma unroll
         for (int c = 0; c < 36; c++) s[36 + c] += dp6[c] * d.wgt;
     }
-    reduce_store<72, 0>(s, nullptr, d.partials, d.red + OFF_C0, d.counters + CNT_C0);
+    reduce_store<72, 0>(s, nullptr, d.partials, d.red + OFF_C0, d.counters + CNT_C0, hw_vb());
 }
 void launch_c0(const Dev& d, double tdot, double tdotref, cudaStream_t st) {
     const size_t sm = (size_t)kC0Block * 72 * sizeof(double);
@@ -2235,7 +2244,7 @@ __global__ void __launch_bounds__(kBlock) k_kinematic(Dev d, double tdot_step) {
         m[2] = fmax(m[2], st);
         m[3] = fmax(m[3], -(d.detF[v] * Ji));
     }
-    reduce_store<0, 4>(nullptr, m, d.partials, d.red + OFF_KIN, d.counters + CNT_KIN);
+    reduce_store<0, 4>(nullptr, m, d.partials, d.red + OFF_KIN, d.counters + CNT_KIN, hw_vb());
 }
 void launch_kinematic(const Dev& d, double tdot_step, cudaStream_t st) { k_kinematic<<<d.grid, kBlock, 0, st>>>(d, tdot_step); }
 
@@ -2428,7 +2437,7 @@ __global__ void __launch_bounds__(kBlock) k_goperr0(Dev d, const double* __restr
                 for (int i = 0; i < 3; i++)
                     for (int j = 0; j < 3; j++) s[((p * 3 + q) * 3 + i) * 3 + j] += -a[3 * p + i] * (xi[q] * xi[j]);
     }
-    reduce_store<81, 0>(s, nullptr, d.partials, d.red + OFF_G0, d.counters + CNT_G0);
+    reduce_store<81, 0>(s, nullptr, d.partials, d.red + OFF_G0, d.counters + CNT_G0, hw_vb());
 }
 void launch_goperr0(const Dev& d, const double* c0, const double* s0, int igamma, cudaStream_t st) {
     k_goperr0<<<d.grid, kBlock, 0, st>>>(d, c0, s0, igamma);

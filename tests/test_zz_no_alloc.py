@@ -33,8 +33,9 @@ def _call(fn, tau_dev, out_dev, shape, c0, s0):
 
 
 # 32^3 (power-of-two passes), 24 x 20 x 12 (radix-3/5 stages, a non-cubic box), 8 x 8 x 1 (a 2-D grid)
-# and 30 x 32 x 34, a non-cubic grid at the scratch limit: (30/2 + 1) * 32 * 34 = 17408 half-spectrum points.
-SHAPES = [(32, 32, 32), (24, 20, 12), (8, 8, 1), (30, 32, 34)]
+# and 33 x 32 x 32, a grid with an odd x edge exactly at the scratch limit:
+# (33 / 2 + 1) * 32 * 32 = 17 * 1024 = 17408 half-spectrum points.
+SHAPES = [(32, 32, 32), (24, 20, 12), (8, 8, 1), (33, 32, 32)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
