@@ -19,7 +19,10 @@ OUT = PKG / "_build"
 LIB = OUT / "libevp_b200.so"
 INCLUDE = PKG.parent / "include"
 
-SOURCES = ["evp_solver.cu", "evp_kernels.cu", "evp_fft.cu", "evp_green.cu", "evp_deck.cpp", "evp_server.cpp"]
+SOURCES = ["evp_solver.cu", "evp_engine.cu", "evp_control.cu", "evp_kernels.cu", "evp_fft.cu", "evp_green.cu",
+           "evp_deck.cpp", "evp_server.cpp"]
+# per-file extra flags: the device-side iteration tail keeps plain multiply-then-add rounding
+EXTRA_FLAGS = {"evp_control.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", f"-I{INCLUDE}"]
 
@@ -53,7 +56,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         obj = OUT / (name + ".o")
         objs.append(obj)
         if force or _stale(obj, src):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *EXTRA_FLAGS.get(name, []), "-c", str(src), "-o", str(obj)]
             if name.endswith(".cpp"):
                 cmd = [nvcc, "-x", "cu", *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
             jobs.append(cmd)

@@ -130,6 +130,99 @@ struct Upd3Params {
     long long vlast;  // last solid voxel in loop order (for the eelav quirk, LS-EVPFFT.f90:482-483)
 };
 
+// Control block of one solve's equilibrium iteration, in device memory.  The host
+// fills it at the start of an increment (and after a sub-step restart); the
+// iteration kernels read their parameters from it; k_control, run after every
+// iteration, does the serial tail of the reference's loop on the device (the
+// averages and the boundary-condition update of calc_velgradavg_corr and
+// state_6x6_evpsc, the error norms, the mixing factor, the convergence test and
+// the time-step rules, LS-EVPFFT.f90:277-430) and stops the solve's iteration
+// with an event code the host reads, so that no iteration waits for the host.
+enum : int { EV_RUNNING = 0, EV_CONVERGED = 1, EV_ACCEPTED = 2, EV_HOST = 3 };
+struct IterCtl {
+    // read by the iteration kernels
+    int active;  // 1 while this solve iterates; 0 once k_control has set an event
+    int prec;    // spectrum precision of the next iteration: 0 FP64, 1 FP32
+    int fresh;   // the next iteration is the first of its increment: form the stress average first
+    int sg_off;  // where the PK1 prologue reads the average stress (OFF_SGAVG or OFF_NEWTON + 8)
+    CorrParams corr;
+    XinvParams xinv;
+    NewtonParams newton;
+    // iteration state
+    int iter, itmax, ictrl, event;  // event: EV_* or a negative status code
+    int errbits, kinematic, did_converge, nhist;
+    long long total_iters;
+    double error, tdotmin, devmapp, lvmavg;
+    double erre, errs, errsbc, svmavg, wphcsol, wphcgas;
+    double hist[4];  // the last four error maxima of the FP32 iterations (ring)
+    double velgradavg[9], velgradavggas[9], velgradavgsol[9], sgavg[9], sgavgsol[9];
+    double de_ds[81];
+    // boundary conditions of the current process (dsim and scauchy change every iteration)
+    int iscau[6], idsim[6], iudot[9];
+    double udot[9], dsim[9], scauchy[9];
+    double tdot, tdotref;
+};
+
+// One member of a batched launch: the solve's device state, its FFT plans, its
+// control block and its reference-medium stiffness / compliance (device arrays).
+struct BatchSolve {
+    Dev d;
+    FftPlan1D pl1, pl2, pl3;
+    IterCtl* ctl;
+    const double* c0;
+    const double* s0;
+};
+// A batched launch covers, for every member it serves, the blocks
+// [blk0, blk0 + gx * gy * gz) of the launch; inside them the member's kernel body
+// sees the solve-local block (b % gx, (b / gx) % gy, b / (gx gy)), exactly the
+// grid and tile its own single-solve launch would use.
+struct Job {
+    int solve, blk0, gx, gy, gz, tile;
+};
+// The passes of one equilibrium iteration, in launch order.
+enum BatchKind : int { BK_SGAVG, BK_XFWD, BK_YFWD, BK_ZGREEN, BK_YINV, BK_XINV, BK_CORR, BK_NEWTON, BK_N };
+struct BatchLaunch {
+    int kind, variant;  // variant: FFT passes rs | (FP32 << 1); Newton: the kernel (newton_variant)
+    int job0, njobs;    // slice of the plan's job table
+    int blocks, threads;
+    size_t smem;
+};
+// Job-table entries of one member for every pass it takes part in (host side of the batch
+// plan): [0] the FP64 launch shape of each pass, [1] the FP32 one of the spectral passes of a
+// mixed-precision member (has32).
+struct MemberJobs {
+    Job job[2][BK_N];
+    int variant[2][BK_N];
+    int threads[2][BK_N];
+    size_t smem[2][BK_N];
+    bool has32;
+};
+
+#ifdef __CUDACC__
+// Block side of a batched launch: the member whose job covers this block (binary search on
+// blk0), the member's descriptor copied to shared memory, and the solve-local block.
+static_assert(sizeof(BatchSolve) % 8 == 0, "BatchSolve is copied in 8-byte words");
+__device__ __forceinline__ Job batch_job(const Job* __restrict__ jobs, int njobs) {
+    int lo = 0, hi = njobs - 1;
+    const int b = blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].blk0 <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return jobs[lo];
+}
+__device__ __forceinline__ void load_member(BatchSolve& dst, const BatchSolve* __restrict__ src) {
+    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* b = reinterpret_cast<unsigned long long*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(BatchSolve) / 8); i += blockDim.x) b[i] = a[i];
+}
+__device__ __forceinline__ VB job_vb(const Job& jb) {
+    const int l = (int)blockIdx.x - jb.blk0;
+    return VB{l % jb.gx, (l / jb.gx) % jb.gy, l / (jb.gx * jb.gy), jb.gx};
+}
+#endif
+
 // ---- launch wrappers (stream-ordered)
 // keepF: F, F^-1, det F and the unscaled weights w J were set by launch_dispini; the weights
 // are divided by detFavg here (IO_functions.f90:934) and weight the start-up tangent sum
@@ -153,6 +246,15 @@ void launch_diag(const Dev& d, double Lfloor, cudaStream_t st);
 void launch_c0(const Dev& d, double tdot, double tdotref, cudaStream_t st);
 void launch_kinematic(const Dev& d, double tdot_step, cudaStream_t st);
 void launch_cell2node(const Dev& d, double tdot, int ideriv, cudaStream_t st);
+
+// Batched equilibrium iteration: the member's per-pass launch shape (its single-solve grid
+// and tile) and the launches over a job table (E, jobs: device arrays).
+void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj);
+void member_jobs_fft(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, int prec, MemberJobs& mj);
+void launch_batched_voxel(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st);
+void launch_batched_fft(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st);
+// the serial tail of one iteration for n solves (evp_control.cu); events[i] = EV_* or a status code
+void launch_control(const BatchSolve* E, int n, int* events, cudaStream_t st);
 
 // FFT engine (evp_fft.cu)
 FftPlan1D make_plan(int n);

@@ -838,8 +838,15 @@ void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
     else green_apply_rs<1>(d, pl1, pl2, pl3, tau, out, c0, s0, st);
 }
 
+// Launch shape of one pass over one solve: grid (gx, gy, gz), tile (rows or pencils per
+// block), threads per block and dynamic shared memory.  The single-solve launchers and the
+// batched launches use the same shapes, so a solve's blocks do the same work either way.
+struct FftShape {
+    int gx, gy, gz, tile, thr;
+    size_t smem;
+};
 template <int RS, class CT>
-static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
+static FftShape x_fwd_shape(const Dev& d, const FftPlan1D& pl) {
     static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS, CT>);
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
@@ -847,9 +854,12 @@ static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cu
                               [&](int g) { return (npr + g - 1) / g; },
                               [&](int g) { return (size_t)9 * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
-    const int grid = (npairs + G - 1) / G;
-    const size_t smem = (size_t)9 * G * d.n1 * sizeof(CT);
-    k_fft_x_fwd<RS, CT><<<grid, thr, smem, st>>>(d, pl, G, mode, sg_off);
+    return FftShape{(npairs + G - 1) / G, 1, 1, G, thr, (size_t)9 * G * d.n1 * sizeof(CT)};
+}
+template <int RS, class CT>
+static void x_fwd_rs(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st) {
+    const FftShape sh = x_fwd_shape<RS, CT>(d, pl);
+    k_fft_x_fwd<RS, CT><<<sh.gx, sh.thr, sh.smem, st>>>(d, pl, sh.tile, mode, sg_off);
 }
 void launch_fft_x_fwd(const Dev& d, const FftPlan1D& pl, int mode, int sg_off, cudaStream_t st, int prec) {
     const bool f32 = prec != 0 && mode == 0;  // the grid-update chain (mode 1) stays FP64
@@ -864,16 +874,20 @@ static int y_tile(const Dev& d) {
     return (d.n1h + nt - 1) / nt;
 }
 template <int RS, class CT>
-static void y_rs(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
+static FftShape y_shape(const Dev& d, const FftPlan1D& pl, int ncomp) {
     static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS, CT>), kernel_max_threads((const void*)k_fft_y<false, RS, CT>));
     int thr = 0;
     const int T = choose_tile((const void*)k_fft_y<false, RS, CT>, y_tile(d), 1, pl, RS, 64, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n3 * ncomp; },
                               [&](int t) { return (size_t)t * d.n2 * sizeof(CT); }, thr);
-    dim3 grid((d.n1h + T - 1) / T, d.n3, ncomp);
-    const size_t smem = (size_t)T * d.n2 * sizeof(CT);
-    if (inverse) k_fft_y<true, RS, CT><<<grid, thr, smem, st>>>(d, pl, T);
-    else k_fft_y<false, RS, CT><<<grid, thr, smem, st>>>(d, pl, T);
+    return FftShape{(d.n1h + T - 1) / T, d.n3, ncomp, T, thr, (size_t)T * d.n2 * sizeof(CT)};
+}
+template <int RS, class CT>
+static void y_rs(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st) {
+    const FftShape sh = y_shape<RS, CT>(d, pl, ncomp);
+    dim3 grid(sh.gx, sh.gy, sh.gz);
+    if (inverse) k_fft_y<true, RS, CT><<<grid, sh.thr, sh.smem, st>>>(d, pl, sh.tile);
+    else k_fft_y<false, RS, CT><<<grid, sh.thr, sh.smem, st>>>(d, pl, sh.tile);
 }
 void launch_fft_y(const Dev& d, const FftPlan1D& pl, int ncomp, bool inverse, cudaStream_t st, int prec) {
     if (plan_pow2(pl)) prec ? y_rs<0, float2>(d, pl, ncomp, inverse, st) : y_rs<0, double2>(d, pl, ncomp, inverse, st);
@@ -887,15 +901,18 @@ static int z_tile(const Dev& d) {
     return (d.n1h + nt - 1) / nt;
 }
 template <int RS, class CT>
-static void z_green_rs(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
+static FftShape z_green_shape(const Dev& d, const FftPlan1D& pl) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS, CT>);
     int thr = 0;
     const int T = choose_tile((const void*)k_fft_z_green<RS, CT>, z_tile(d), 9, pl, RS, 128, mx,
                               [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
                               [&](int t) { return (size_t)9 * t * d.n3 * sizeof(CT); }, thr);
-    dim3 grid((d.n1h + T - 1) / T, d.n2);
-    const size_t smem = (size_t)9 * T * d.n3 * sizeof(CT);
-    k_fft_z_green<RS, CT><<<grid, thr, smem, st>>>(d, pl, T, c0, s0);
+    return FftShape{(d.n1h + T - 1) / T, d.n2, 1, T, thr, (size_t)9 * T * d.n3 * sizeof(CT)};
+}
+template <int RS, class CT>
+static void z_green_rs(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st) {
+    const FftShape sh = z_green_shape<RS, CT>(d, pl);
+    k_fft_z_green<RS, CT><<<dim3(sh.gx, sh.gy), sh.thr, sh.smem, st>>>(d, pl, sh.tile, c0, s0);
 }
 void launch_fft_z_green(const Dev& d, const FftPlan1D& pl, const double* c0, const double* s0, cudaStream_t st, int prec) {
     if (plan_pow2(pl)) prec ? z_green_rs<0, float2>(d, pl, c0, s0, st) : z_green_rs<0, double2>(d, pl, c0, s0, st);
@@ -950,23 +967,135 @@ void launch_gradient(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, c
     else gradient_rs<1>(d, pl1, pl2, pl3, u9, out, ideriv, st);
 }
 template <int RS, class CT>
-static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
+static FftShape x_inv_shape(const Dev& d, const FftPlan1D& pl, int ncomp) {
     static const int mx = kernel_max_threads((const void*)k_fft_x_inv<RS, CT>);
-    const int ncomp = (mode == 0) ? 9 : 3;
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
     const int G = choose_tile((const void*)k_fft_x_inv<RS, CT>, x_rows_per_block(d.n1), ncomp, pl, RS, 128, mx,
                               [&](int g) { return (npr + g - 1) / g; },
                               [&](int g) { return (size_t)ncomp * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
-    const int grid = (npairs + G - 1) / G;
-    const size_t smem = (size_t)ncomp * G * d.n1 * sizeof(CT);
-    k_fft_x_inv<RS, CT><<<grid, thr, smem, st>>>(d, pl, G, ncomp, mode, p);
+    return FftShape{(npairs + G - 1) / G, 1, 1, G, thr, (size_t)ncomp * G * d.n1 * sizeof(CT)};
+}
+template <int RS, class CT>
+static void x_inv_rs(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st) {
+    const int ncomp = (mode == 0) ? 9 : 3;
+    const FftShape sh = x_inv_shape<RS, CT>(d, pl, ncomp);
+    k_fft_x_inv<RS, CT><<<sh.gx, sh.thr, sh.smem, st>>>(d, pl, sh.tile, ncomp, mode, p);
 }
 void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvParams& p, cudaStream_t st, int prec) {
     const bool f32 = prec != 0 && mode == 0;  // the grid-update chain (mode 1) stays FP64
     if (plan_pow2(pl)) f32 ? x_inv_rs<0, float2>(d, pl, mode, p, st) : x_inv_rs<0, double2>(d, pl, mode, p, st);
     else f32 ? x_inv_rs<1, float2>(d, pl, mode, p, st) : x_inv_rs<1, double2>(d, pl, mode, p, st);
+}
+
+// ---------------------------------------------------------------- batched launches of the iteration's spectral passes
+// As the voxel passes (evp_kernels.cu): each block finds its member, copies the member's
+// descriptor to shared memory and runs the member's body on its own block coordinates.
+// A member takes part in the FP64 launch of a pass while its control block asks for FP64
+// spectra and in the FP32 launch while it asks for FP32 (mixed precision).
+template <class CT>
+__device__ __forceinline__ bool batch_go(const IterCtl* c) {
+    return c->active && ((c->prec != 0) == (sizeof(CT) == sizeof(float2)));
+}
+template <int RS, class CT>
+__global__ void __launch_bounds__(256, 2) kb_fft_x_fwd(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ int go, sg_off;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) {
+        const IterCtl* c = E[jb.solve].ctl;
+        go = batch_go<CT>(c);
+        sg_off = c->sg_off;
+    }
+    __syncthreads();
+    if (!go) return;
+    body_fft_x_fwd<RS, CT>(m.d, m.pl1, jb.tile, 0, sg_off, job_vb(jb));
+}
+template <bool INV, int RS, class CT>
+__global__ void __launch_bounds__(256, 2) kb_fft_y(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ int go;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) go = batch_go<CT>(E[jb.solve].ctl);
+    __syncthreads();
+    if (!go) return;
+    body_fft_y<INV, RS, CT>(m.d, m.pl2, jb.tile, job_vb(jb));
+}
+template <int RS, class CT>
+__global__ void __launch_bounds__(256, 2) kb_fft_z_green(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ int go;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) go = batch_go<CT>(E[jb.solve].ctl);
+    __syncthreads();
+    if (!go) return;
+    body_fft_z_green<RS, CT>(m.d, m.pl3, jb.tile, m.c0, m.s0, job_vb(jb));
+}
+template <int RS, class CT>
+__global__ void __launch_bounds__(256, 2) kb_fft_x_inv(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ XinvParams xp;
+    __shared__ int go;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) {
+        const IterCtl* c = E[jb.solve].ctl;
+        go = batch_go<CT>(c);
+        xp = c->xinv;
+    }
+    __syncthreads();
+    if (!go) return;
+    body_fft_x_inv<RS, CT>(m.d, m.pl1, jb.tile, 9, 0, xp, job_vb(jb));
+}
+
+template <class CT>
+static void member_fft_ct(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, int w,
+                          MemberJobs& mj) {
+    // the radix set of each pass follows its own axis, as in the single-solve launchers
+    const int rs1 = plan_pow2(pl1) ? 0 : 1, rs2 = plan_pow2(pl2) ? 0 : 1, rs3 = plan_pow2(pl3) ? 0 : 1;
+    auto put = [&](int k, const FftShape& sh, int rs) {
+        mj.job[w][k] = Job{0, 0, sh.gx, sh.gy, sh.gz, sh.tile};
+        mj.threads[w][k] = sh.thr;
+        mj.smem[w][k] = sh.smem;
+        mj.variant[w][k] = rs | (w << 1);
+    };
+    put(BK_XFWD, rs1 ? x_fwd_shape<1, CT>(d, pl1) : x_fwd_shape<0, CT>(d, pl1), rs1);
+    const FftShape y = rs2 ? y_shape<1, CT>(d, pl2, 9) : y_shape<0, CT>(d, pl2, 9);
+    put(BK_YFWD, y, rs2);
+    put(BK_YINV, y, rs2);
+    put(BK_ZGREEN, rs3 ? z_green_shape<1, CT>(d, pl3) : z_green_shape<0, CT>(d, pl3), rs3);
+    put(BK_XINV, rs1 ? x_inv_shape<1, CT>(d, pl1, 9) : x_inv_shape<0, CT>(d, pl1, 9), rs1);
+}
+
+void member_jobs_fft(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, int prec, MemberJobs& mj) {
+    member_fft_ct<double2>(d, pl1, pl2, pl3, 0, mj);
+    if (prec) member_fft_ct<float2>(d, pl1, pl2, pl3, 1, mj);
+    mj.has32 = prec != 0;
+}
+
+template <int RS, class CT>
+static void batched_fft_ct(const BatchLaunch& L, const BatchSolve* E, const Job* J, cudaStream_t st) {
+    switch (L.kind) {
+        case BK_XFWD: kb_fft_x_fwd<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+        case BK_YFWD: kb_fft_y<false, RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+        case BK_ZGREEN: kb_fft_z_green<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+        case BK_YINV: kb_fft_y<true, RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+        case BK_XINV: kb_fft_x_inv<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+        default: break;
+    }
+}
+void launch_batched_fft(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st) {
+    const Job* J = jobs + L.job0;
+    switch (L.variant) {
+        case 0: batched_fft_ct<0, double2>(L, E, J, st); break;
+        case 1: batched_fft_ct<1, double2>(L, E, J, st); break;
+        case 2: batched_fft_ct<0, float2>(L, E, J, st); break;
+        default: batched_fft_ct<1, float2>(L, E, J, st); break;
+    }
 }
 
 // Raise the dynamic shared-memory limit of the FFT kernels (once per process).
@@ -978,6 +1107,11 @@ static void configure_ct() {
     cudaFuncSetAttribute(k_fft_y<true, RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(k_fft_z_green<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(k_fft_x_inv<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(kb_fft_x_fwd<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(kb_fft_y<false, RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(kb_fft_y<true, RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(kb_fft_z_green<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(kb_fft_x_inv<RS, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 template <int RS>
 static void configure_rs() {

@@ -25,6 +25,8 @@
 #include "evp_math.cuh"
 
 #include <cstdio>
+#include <cstdlib>
+#include <mutex>
 
 namespace evp {
 
@@ -561,12 +563,12 @@ __device__ __forceinline__ void harden(const PhaseDev& ph, const double* __restr
 
 // ---------------------------------------------------------------- k_newton
 template <int NS>
-__global__ void __launch_bounds__(kNewtonBlock, 2) k_newton(Dev d, NewtonParams p) {
+__device__ __forceinline__ void body_newton1(const Dev& d, const NewtonParams& p, const VB& vb) {
     const long long N = d.N;
     double s[14];
 #pragma unroll
     for (int c = 0; c < 14; c++) s[c] = 0.0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+    for (long long v = vb.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)vb.nx * blockDim.x) {
         double lam[6], sg[6], sgt[6], D[6];
         {
             double vg[9], vs[9], a[6];
@@ -760,8 +762,10 @@ __global__ void __launch_bounds__(kNewtonBlock, 2) k_newton(Dev d, NewtonParams 
             s[8 + c] += s6v[c] * w;
         }
     }
-    reduce_store<14, 0>(s, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON, hw_vb());
+    reduce_store<14, 0>(s, nullptr, d.partials, d.red + OFF_NEWTON, d.counters + CNT_NEWTON, vb);
 }
+template <int NS>
+__global__ void __launch_bounds__(kNewtonBlock, 2) k_newton(Dev d, NewtonParams p) { body_newton1<NS>(d, p, hw_vb()); }
 // ---------------------------------------------------------------- k_newton6: six lanes per voxel
 // The local solve of k_newton with the voxel's operators held in registers for
 // the whole Newton solve instead of being re-read from memory at every
@@ -1739,47 +1743,164 @@ __device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& 
 template <int SPL>
 __global__ void __launch_bounds__(256, 2) k_newton6p(Dev d, NewtonParams p) { body_newton6p<SPL>(d, p, hw_vb()); }
 
-void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
-    // EVP_NEWTON_ONE_THREAD=1 selects the one-thread-per-voxel kernel, kept for comparison
+// The local-solve kernel of a solve: 0 k_newton6p<2>, 1 k_newton6p<4> (symmetric form, no modAL,
+// at most kMaxPhaseSmem phases), 2/3 k_newton6<2/4, modal>, 4/5 k_newton6<2/4, no modAL>, and
+// 6/7 the one-thread-per-voxel kernel k_newton<12/24> (EVP_NEWTON_ONE_THREAD=1, kept for comparison).
+static int newton_variant(const Dev& d, int modal) {
     static const bool one_thread = [] {
         const char* e = getenv("EVP_NEWTON_ONE_THREAD");
         return e && e[0] == '1';
     }();
     const bool big = d.nsys > 12;
-    if (one_thread) {
-        int grid = (int)((d.N + kNewtonBlock - 1) / kNewtonBlock);
-        if (grid > 148 * 16) grid = 148 * 16;
-        if (big) k_newton<24><<<grid, kNewtonBlock, 0, st>>>(d, p);
-        else k_newton<12><<<grid, kNewtonBlock, 0, st>>>(d, p);
-        return;
+    if (one_thread) return big ? 7 : 6;
+    if (!modal && d.nph <= kMaxPhaseSmem) return big ? 1 : 0;
+    if (modal) return big ? 3 : 2;
+    return big ? 5 : 4;
+}
+static int newton_grid(const Dev& d, int variant) {
+    if (variant >= 6) {
+        const long long g = (d.N + kNewtonBlock - 1) / kNewtonBlock;
+        return (int)(g < 148LL * 16 ? g : 148LL * 16);
     }
     const long long warps = (d.N + 4) / 5;
     const long long g = (warps + 7) / 8;  // 8 warps per block of 256
-    const int grid = (int)(g < 148LL * 24 ? g : 148LL * 24);
-    if (!p.modal && d.nph <= kMaxPhaseSmem) {
-        const size_t sm = newton6p_smem_bytes(big ? 4 : 2, d.nph);
-        if (big) {
-            cudaFuncSetAttribute(k_newton6p<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_newton6p<4><<<grid, 256, sm, st>>>(d, p);
-        } else {
-            cudaFuncSetAttribute(k_newton6p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_newton6p<2><<<grid, 256, sm, st>>>(d, p);
-        }
-        return;
+    return (int)(g < 148LL * 24 ? g : 148LL * 24);
+}
+static size_t newton_smem(const Dev& d, int variant) {
+    switch (variant) {
+        case 0: return newton6p_smem_bytes(2, d.nph);
+        case 1: return newton6p_smem_bytes(4, d.nph);
+        case 2: case 4: return newton6_smem_bytes(2);
+        case 3: case 5: return newton6_smem_bytes(4);
+        default: return 0;
     }
-    const size_t sm6 = newton6_smem_bytes(big ? 4 : 2);
-    if (p.modal) {
-        if (big) k_newton6<4, true><<<grid, 256, sm6, st>>>(d, p);
-        else {
-            cudaFuncSetAttribute(k_newton6<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
-            k_newton6<2, true><<<grid, 256, sm6, st>>>(d, p);
-        }
-    } else {
-        if (big) k_newton6<4, false><<<grid, 256, sm6, st>>>(d, p);
-        else {
-            cudaFuncSetAttribute(k_newton6<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm6);
-            k_newton6<2, false><<<grid, 256, sm6, st>>>(d, p);
-        }
+}
+template <int V>
+__global__ void __launch_bounds__(V >= 6 ? 128 : 256, 2) kb_newton(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs,
+                                                                   int njobs);
+static void newton_configure() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const int lim = 200 * 1024;
+        cudaFuncSetAttribute(k_newton6p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(k_newton6p<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(k_newton6<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(k_newton6<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(kb_newton<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(kb_newton<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(kb_newton<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(kb_newton<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(kb_newton<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        cudaFuncSetAttribute(kb_newton<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    });
+}
+
+void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
+    newton_configure();
+    const int v = newton_variant(d, p.modal);
+    const int grid = newton_grid(d, v);
+    const size_t sm = newton_smem(d, v);
+    switch (v) {
+        case 0: k_newton6p<2><<<grid, 256, sm, st>>>(d, p); break;
+        case 1: k_newton6p<4><<<grid, 256, sm, st>>>(d, p); break;
+        case 2: k_newton6<2, true><<<grid, 256, sm, st>>>(d, p); break;
+        case 3: k_newton6<4, true><<<grid, 256, sm, st>>>(d, p); break;
+        case 4: k_newton6<2, false><<<grid, 256, sm, st>>>(d, p); break;
+        case 5: k_newton6<4, false><<<grid, 256, sm, st>>>(d, p); break;
+        case 6: k_newton<12><<<grid, kNewtonBlock, 0, st>>>(d, p); break;
+        default: k_newton<24><<<grid, kNewtonBlock, 0, st>>>(d, p); break;
+    }
+}
+
+// ---------------------------------------------------------------- batched launches of the iteration's voxel passes
+// Each block finds its member in the job table (binary search on blk0), copies the
+// member's descriptor to shared memory, reads its control block and runs the same
+// body as the member's single-solve launch, on the member's own block coordinates.
+// Blocks of members that are not iterating (converged, waiting for the host) exit.
+__global__ void __launch_bounds__(kBlock) kb_sgavg(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ int go;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) {
+        const IterCtl* c = E[jb.solve].ctl;
+        go = c->active && c->fresh;
+    }
+    __syncthreads();
+    if (!go) return;
+    body_sgavg(m.d, job_vb(jb));
+}
+__global__ void __launch_bounds__(kBlock, 2) kb_corr(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ CorrParams p;
+    __shared__ int go;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) {
+        const IterCtl* c = E[jb.solve].ctl;
+        go = c->active;
+        p = c->corr;
+    }
+    __syncthreads();
+    if (!go) return;
+    body_corr(m.d, p, job_vb(jb));
+}
+template <int V>
+__global__ void __launch_bounds__(V >= 6 ? kNewtonBlock : 256, 2) kb_newton(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
+    __shared__ BatchSolve m;
+    __shared__ NewtonParams p;
+    __shared__ int go;
+    const Job jb = batch_job(jobs, njobs);
+    load_member(m, E + jb.solve);
+    if (threadIdx.x == 0) {
+        const IterCtl* c = E[jb.solve].ctl;
+        go = c->active;
+        p = c->newton;
+    }
+    __syncthreads();
+    if (!go) return;
+    const VB vb = job_vb(jb);
+    if constexpr (V == 0) body_newton6p<2>(m.d, p, vb);
+    else if constexpr (V == 1) body_newton6p<4>(m.d, p, vb);
+    else if constexpr (V == 2) body_newton6<2, true>(m.d, p, vb);
+    else if constexpr (V == 3) body_newton6<4, true>(m.d, p, vb);
+    else if constexpr (V == 4) body_newton6<2, false>(m.d, p, vb);
+    else if constexpr (V == 5) body_newton6<4, false>(m.d, p, vb);
+    else if constexpr (V == 6) body_newton1<12>(m.d, p, vb);
+    else body_newton1<24>(m.d, p, vb);
+}
+void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj) {
+    newton_configure();
+    auto one_d = [&](int k, int grid, int thr, size_t sm, int variant) {
+        mj.job[0][k] = Job{0, 0, grid, 1, 1, 0};
+        mj.threads[0][k] = thr;
+        mj.smem[0][k] = sm;
+        mj.variant[0][k] = variant;
+    };
+    one_d(BK_SGAVG, d.grid, kBlock, 0, 0);
+    one_d(BK_CORR, d.grid < 148 * 2 ? d.grid : 148 * 2, kBlock, 0, 0);
+    const int v = newton_variant(d, modal);
+    one_d(BK_NEWTON, newton_grid(d, v), v >= 6 ? kNewtonBlock : 256, newton_smem(d, v), v);
+}
+
+void launch_batched_voxel(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st) {
+    const Job* J = jobs + L.job0;
+    switch (L.kind) {
+        case BK_SGAVG: kb_sgavg<<<L.blocks, L.threads, 0, st>>>(E, J, L.njobs); break;
+        case BK_CORR: kb_corr<<<L.blocks, L.threads, 0, st>>>(E, J, L.njobs); break;
+        case BK_NEWTON:
+            switch (L.variant) {
+                case 0: kb_newton<0><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 1: kb_newton<1><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 2: kb_newton<2><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 3: kb_newton<3><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 4: kb_newton<4><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 5: kb_newton<5><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 6: kb_newton<6><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                default: kb_newton<7><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+            }
+            break;
+        default: break;
     }
 }
 

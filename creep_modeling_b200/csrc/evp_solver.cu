@@ -9,6 +9,7 @@
 #include "../../include/evp.h"
 #include "evp_deck.h"
 #include "evp_dev.cuh"
+#include "evp_engine.h"
 #include "evp_math.cuh"
 
 #include <cuda_runtime.h>
@@ -16,7 +17,9 @@
 #include <algorithm>
 #include <chrono>
 #include <filesystem>
+#include <functional>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <cstdio>
@@ -31,10 +34,6 @@ namespace evp {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& m) { g_last_error = m; }
 
-struct SolveError : std::runtime_error {
-    int code;
-    SolveError(const std::string& m, int c) : std::runtime_error(m), code(c) {}
-};
 
 #define CK(x)                                                                                              \
     do {                                                                                                   \
@@ -99,6 +98,10 @@ public:
     std::vector<void*> allocs;
     double* h_red = nullptr;  // pinned copy of the result buffer
     int* h_err = nullptr;
+    IterCtl* d_ctl = nullptr;  // control block of the equilibrium iteration (device) and its pinned host copy
+    IterCtl* h_ctl = nullptr;
+    bool own_stream = true;
+    bool did_converge = false, accept_step = false;
     double *d_c0 = nullptr, *d_s0 = nullptr, *d_g0 = nullptr;
     // macro state (micro_type, types.f90:55-94)
     double c066[36] = {}, s066[36] = {}, c0[81] = {}, s0[81] = {}, de_ds[81] = {}, goperr0[81] = {};
@@ -139,18 +142,25 @@ public:
         void* p = nullptr;
         if (n == 0) return nullptr;
         // stream-ordered from the library's own pool: no device-wide sync, so concurrent solves do not stall
-        CK(cudaMallocFromPoolAsync(&p, n * sizeof(T), solver_pool(), st));
+        CK(cudaMallocFromPoolAsync(&p, n * sizeof(T), evp::solver_pool(), st));
         allocs.push_back(p);
         return (T*)p;
     }
     ~Solver() {
+        solo.reset();
         for (void* p : allocs) cudaFreeAsync(p, st);
         if (st) cudaStreamSynchronize(st);
         if (h_red) cudaFreeHost(h_red);
         if (h_err) cudaFreeHost(h_err);
+        if (h_ctl) cudaFreeHost(h_ctl);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        if (st) cudaStreamDestroy(st);
+        if (st && own_stream) cudaStreamDestroy(st);
+        for (auto& p : pend) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        for (auto e : evpool) cudaEventDestroy(e);
     }
 
     // ---- host<->device byte counters and the optional per-kernel event timer
@@ -210,46 +220,32 @@ public:
     }
 
     void sync() { CK(cudaStreamSynchronize(st)); }
-    void fetch_red() {
+    // the result buffer and the error word to the host: queued (fetch_red_async), then read after
+    // the stream is synchronised (check_red); fetch_red does both
+    void fetch_red_async() {
         CK(cudaMemcpyAsync(h_red, d.red, RED_OUT_SIZE * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(h_err, d.err, sizeof(int), cudaMemcpyDeviceToHost, st));
         d2h += RED_OUT_SIZE * sizeof(double) + sizeof(int);
-        sync();
+    }
+    void check_red() {
         resolve_timers();
         if (*h_err & 1) throw SolveError("singular matrix in a voxel operator (lu_inverse / lu_eqsystem)", -3);
         if (*h_err & 2) throw SolveError("non-finite stress in the local Newton solve", -4);
         if (*h_err & 4) throw SolveError("form_G failed (singular acoustic tensor or complex D operator)", -3);
     }
-
-    // The solver allocates stream-ordered from a memory pool of its own, one per device, that
-    // keeps freed memory instead of handing it back to the driver at every synchronisation:
-    // back-to-back and concurrent solves then reuse it rather than mapping ~2 kB per voxel
-    // afresh.  The device's default pool, which the embedding application (PyTorch's
-    // cudaMallocAsync backend, say) may use, is left as it is.  The pool's memory stays
-    // with this process until it exits.
-    static cudaMemPool_t solver_pool() {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess) throw SolveError("cudaGetDevice failed", -6);
-        static std::mutex m;
-        static std::map<int, cudaMemPool_t> pools;
-        std::lock_guard<std::mutex> lk(m);
-        auto it = pools.find(dev);
-        if (it != pools.end()) return it->second;
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.handleTypes = cudaMemHandleTypeNone;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t pool;
-        CK(cudaMemPoolCreate(&pool, &props));
-        unsigned long long keep = ~0ull;
-        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        pools.emplace(dev, pool);
-        return pool;
+    void fetch_red() {
+        fetch_red_async();
+        sync();
+        check_red();
     }
 
+    // Device memory comes stream-ordered from the library's own pool (solver_pool): no
+    // device-wide synchronisation, so solves running beside each other do not stall, and
+    // back-to-back solves reuse the memory.
+
     // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
-    void open(const std::string& fft_in, const std::string& out, int mix_flag, int modal_flag, int flags) {
+    void open(const std::string& fft_in, const std::string& out, int mix_flag, int modal_flag, int flags,
+              cudaStream_t ext_stream = nullptr) {
         write_files = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) != 0;
         write_vtk_files = (flags & EVP_WRITE_FILES) != 0;
         profile = (flags & EVP_PROFILE) != 0;
@@ -274,7 +270,12 @@ public:
         }
         int dev_count = 0;
         if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) throw SolveError("no CUDA device available", -6);
-        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        if (ext_stream) {
+            st = ext_stream;
+            own_stream = false;
+        } else {
+            CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        }
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
         static std::once_flag configured;
@@ -358,6 +359,10 @@ public:
         CK(cudaMemsetAsync(d_g0, 0, 81 * sizeof(double), st));
         CK(cudaMallocHost(&h_red, RED_OUT_SIZE * sizeof(double)));
         CK(cudaMallocHost(&h_err, sizeof(int)));
+        CK(cudaMallocHost(&h_ctl, sizeof(IterCtl)));
+        std::memset(h_ctl, 0, sizeof(IterCtl));
+        d_ctl = dalloc<IterCtl>(1);
+        CK(cudaMemsetAsync(d_ctl, 0, sizeof(IterCtl), st));
         pl1 = make_plan(dk.n1); pl2 = make_plan(dk.n2); pl3 = make_plan(dk.n3);
         auto twiddles = [&](int n, double2* dst) {
             std::vector<double2> t(n);
@@ -529,143 +534,180 @@ public:
         }
     }
 
-    // ------------------------------------------------------------ state_6x6_evpsc (various_functions.f90:1638-1705)
-    void state_6x6(const int* idsim, double* dbar, const int* iscau, double* sbar, const double* xm, const double* devp0,
-                   double* scauchy, double* dsim) {
-        double profac[6], dbarv[6], sbarv[6], devp0v[6], aux6[6], aux6a[6], a4[81], xmv[36], a33[9], A[36];
-        for (int i = 1; i <= 6; i++) profac[i - 1] = 1.0 + (i / 4);
+    // ------------------------------------------------------------ the increment's iteration control block
+    // Fill the control block for the first iteration of an increment (the iter == 0 block of
+    // LS-EVPFFT.f90:233-240, and what equilibrium_iteration reads from the driver) and upload it.
+    void start_iterations() {
+        ProcessData& p = P();
+        if (dk.has_gas) K("k_gas_compl", [&] { launch_gas_compl(d, p.tdot, dk.complgas, modal ? 1 : 0, st); });
+        std::memset(dvelgradavg, 0, sizeof(dvelgradavg));
+        edotvmmx = 0;
+        mix = 1.0;
+        erre = 2.0 * p.error;
+        errs = 2.0 * p.error;
+        errsbc = 2.0 * p.error;
+        prec_it = prec;
+        IterCtl& c = *h_ctl;
+        std::memset(&c, 0, sizeof(c));
+        c.active = 1;
+        c.prec = prec;
+        c.fresh = 1;
+        c.sg_off = OFF_SGAVG;
+        c.corr.mix = mix;
+        c.corr.Lscale = std::max(lvmavg, EVP_TINY);
+        c.corr.do_mix = do_mix ? 1 : 0;
+        c.corr.kinematic = kinematic ? 1 : 0;
+        if (inv3(dinvc, c.xinv.dinv) != 0) throw SolveError("Singular matrix in lu_inverse (correction_to_current)", -3);
+        c.newton.tdot = p.tdot;
+        c.newton.error = p.error;
+        c.newton.erroral = p.erroral;
+        c.newton.complgas = dk.complgas;
+        c.newton.modal = modal ? 1 : 0;
+        c.newton.thermo = (imicro == 1 && p.ithermo == 1) ? 1 : 0;
+        c.newton.iuphard = p.iuphard;
+        c.iter = 0;
+        c.itmax = p.itmax;
+        c.ictrl = p.ictrl;
+        c.kinematic = kinematic ? 1 : 0;
+        c.total_iters = total_iters;
+        c.error = p.error;
+        c.tdotmin = p.tdotmin;
+        c.devmapp = p.devmapp;
+        c.lvmavg = lvmavg;
+        c.erre = erre;
+        c.errs = errs;
+        c.errsbc = errsbc;
+        c.svmavg = svmavg;
+        c.wphcsol = wphcsol;
+        c.wphcgas = wphcgas;
+        std::memcpy(c.velgradavg, velgradavg, sizeof(velgradavg));
+        std::memcpy(c.de_ds, de_ds, sizeof(de_ds));
         for (int i = 0; i < 6; i++) {
-            dbarv[i] = dsim[3 * ijv_a(i) + ijv_b(i)];
-            sbarv[i] = scauchy[3 * ijv_a(i) + ijv_b(i)];
+            c.iscau[i] = p.iscau[i];
+            c.idsim[i] = p.idsim[i];
         }
-        b66_to_t4(xm, a4);
-        for (int i = 0; i < 6; i++)
-            for (int j = 0; j < 6; j++) xmv[6 * i + j] = a4[(3 * ijv_a(i) + ijv_b(i)) * 9 + 3 * ijv_a(j) + ijv_b(j)];
-        b6_to_t2(devp0, a33);
-        for (int i = 0; i < 6; i++) devp0v[i] = a33[3 * ijv_a(i) + ijv_b(i)];
-        for (int i = 0; i < 6; i++) aux6[i] = dbarv[i] - devp0v[i];
-        for (int i = 0; i < 6; i++) {
-            aux6a[i] = -1.0 * idsim[i] * aux6[i];
-            for (int j = 0; j < 6; j++) {
-                aux6a[i] = aux6a[i] + xmv[6 * i + j] * iscau[j] * sbarv[j] * profac[j];
-                A[6 * i + j] = iscau[j] * (i == j ? 1 : 0) - idsim[j] * xmv[6 * i + j] * profac[j];
-            }
+        for (int k = 0; k < 9; k++) {
+            c.iudot[k] = p.iudot[k];
+            c.udot[k] = p.udot[k];
+            c.dsim[k] = p.dsim[k];
+            c.scauchy[k] = p.scauchy[k];
         }
-        int piv[6];
-        if (lu_factor(A, 6, piv) != 0) throw SolveError("Failed system solve in lu_eqsystem (state_6x6_evpsc)", -3);
-        lu_solve(A, 6, piv, aux6a);
-        for (int i = 0; i < 6; i++) {
-            aux6[i] = idsim[i] * aux6[i] + iscau[i] * aux6a[i];
-            sbarv[i] = iscau[i] * sbarv[i] + idsim[i] * aux6a[i];
-        }
-        for (int i = 0; i < 6; i++) dbarv[i] = aux6[i] + devp0v[i];
-        for (int i = 0; i < 6; i++) {
-            dsim[3 * ijv_a(i) + ijv_b(i)] = dbarv[i];
-            dsim[3 * ijv_b(i) + ijv_a(i)] = dbarv[i];
-            scauchy[3 * ijv_a(i) + ijv_b(i)] = sbarv[i];
-            scauchy[3 * ijv_b(i) + ijv_a(i)] = sbarv[i];
-        }
-        t2_to_b6(dsim, dbar);
-        t2_to_b6(scauchy, sbar);
+        c.tdot = p.tdot;
+        c.tdotref = p.tdotref;
+        h2d_copy(d_ctl, h_ctl, sizeof(IterCtl));
     }
 
-    // ------------------------------------------------------------ calc_velgradavg_corr tail (various_functions.f90:1575-1631)
-    void velgradavg_corr(const double* sgsol6) {
+    // The control block back on the host once the device has stopped the iteration (an event).
+    void pull_ctl() {
+        CK(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(IterCtl), cudaMemcpyDeviceToHost, st));
+        d2h += (long long)sizeof(IterCtl);
+        sync();
+        resolve_timers();
+        const IterCtl& c = *h_ctl;
         ProcessData& p = P();
-        s6_to_t2(sgsol6, sgavg);
-        for (int c = 0; c < 9; c++) sgavgsol[c] = sgavg[c] / wphcsol;
-        svmavg = vm_stress(sgavg);
-        double a33[9];
-        for (int i = 0; i < 6; i++) {
-            int ii = ijv_a(i), jj = ijv_b(i);
-            a33[3 * ii + jj] = p.iscau[i] * (p.scauchy[3 * ii + jj] - sgavg[3 * ii + jj]);
-            a33[3 * jj + ii] = p.iscau[i] * (p.scauchy[3 * jj + ii] - sgavg[3 * jj + ii]);
+        iter = c.iter;
+        total_iters = c.total_iters;
+        erre = c.erre;
+        errs = c.errs;
+        errsbc = c.errsbc;
+        svmavg = c.svmavg;
+        mix = c.corr.mix;
+        prec_it = c.prec;
+        std::memcpy(velgradavg, c.velgradavg, sizeof(velgradavg));
+        std::memcpy(velgradavggas, c.velgradavggas, sizeof(velgradavggas));
+        std::memcpy(velgradavgsol, c.velgradavgsol, sizeof(velgradavgsol));
+        std::memcpy(sgavg, c.sgavg, sizeof(sgavg));
+        std::memcpy(sgavgsol, c.sgavgsol, sizeof(sgavgsol));
+        std::memcpy(dvelgradavg, c.xinv.dvelgradavg, sizeof(dvelgradavg));
+        std::memcpy(p.dsim, c.dsim, sizeof(c.dsim));
+        std::memcpy(p.scauchy, c.scauchy, sizeof(c.scauchy));
+        p.tdot = c.tdot;
+        p.tdotref = c.tdotref;
+        if (verbose) {
+            std::printf("\rMACROSTEP=%d SimTime=%.0fs PROC=%d STEP=%d TDOT=%.0fs ITER=%d", imacroloop, sim_time, ipr, imicro,
+                        p.tdot, iter);
+            std::fflush(stdout);
         }
-        errsbc = frob3(a33);
-        double vsym[9], vasym[9], dbar[6], sbar[6], mev[36], devp0[6];
-        sym33(velgradavg, vsym);
-        antisym33(velgradavg, vasym);
-        t2_to_b6(vsym, dbar);
-        t2_to_b6(sgavg, sbar);
-        t4_to_b66(de_ds, mev);
-        for (int i = 0; i < 6; i++) {
-            double s = 0.0;
-            for (int j = 0; j < 6; j++) s += mev[6 * i + j] * sbar[j];
-            devp0[i] = dbar[i] - s;
-        }
-        state_6x6(p.idsim, dbar, p.iscau, sbar, mev, devp0, p.scauchy, p.dsim);
-        double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int ii = 0; ii < 3; ii++)
-            for (int jj = 0; jj < 3; jj++) {
-                if (ii == jj) { w[3 * ii + jj] = 0.0; continue; }
-                const int a = p.iudot[3 * ii + jj], b = p.iudot[3 * jj + ii];
-                if (a == 1 && b == 0) {
-                    w[3 * ii + jj] = p.udot[3 * ii + jj] - p.dsim[3 * ii + jj];
-                    w[3 * jj + ii] = -w[3 * ii + jj];
-                } else if (a == 0 && b == 1) {
-                } else if (a == 1 && b == 1) {
-                    w[3 * ii + jj] = 0.5 * (p.udot[3 * ii + jj] - p.udot[3 * jj + ii]);
-                } else {
-                    w[3 * jj + ii] = 0.0;
-                }
-            }
-        for (int c = 0; c < 9; c++) dvelgradavg[c] = (p.dsim[c] - vsym[c]) + (w[c] - vasym[c]);
     }
 
-    // ------------------------------------------------------------ one equilibrium iteration (LS-EVPFFT.f90:233-359)
-    void equilibrium_iteration(bool fresh_sgavg) {
+    // Resume the iteration after the host looked at it and changed nothing on the device.
+    void resume_iterations() {
+        h_ctl->active = 1;
+        h_ctl->event = EV_RUNNING;
+        h2d_copy(d_ctl, h_ctl, sizeof(IterCtl));
+    }
+
+    static std::string ctl_message(int bits) {
+        if (bits & 1) return "singular matrix in a voxel operator (lu_inverse / lu_eqsystem)";
+        if (bits & 2) return "non-finite stress in the local Newton solve";
+        if (bits & 4) return "form_G failed (singular acoustic tensor or complex D operator)";
+        if (bits & 8) return "ERRE/ERRS negative -> convergence failed!";
+        if (bits & 16) return "Failed system solve in lu_eqsystem (state_6x6_evpsc)";
+        if (bits & 32) return "equilibrium iteration did not converge";
+        return "equilibrium iteration failed";
+    }
+
+    // After an event: true when the increment's iteration loop is over (converged, or accepted
+    // at ITMAX), false when it goes on (iterations resumed or restarted from the snapshot).
+    // The ictrl = -1 sub-stepping decision of LS-EVPFFT.f90:378-427 runs here.
+    bool handle_event(int ev) {
+        if (ev < 0) throw SolveError(ctl_message(h_ctl->errbits), ev);
         ProcessData& p = P();
-        if (fresh_sgavg) K("k_sgavg", [&] { launch_sgavg(d, st); });
-        K("k_fft_x_fwd", [&] { launch_fft_x_fwd(d, pl1, 0, fresh_sgavg ? OFF_SGAVG : OFF_NEWTON + 8, st, prec_it); });
-        K("k_fft_y_fwd", [&] { launch_fft_y(d, pl2, 9, false, st, prec_it); });
-        K("k_fft_z_green", [&] { launch_fft_z_green(d, pl3, d_c0, d_s0, st, prec_it); });
-        K("k_fft_y_inv", [&] { launch_fft_y(d, pl2, 9, true, st, prec_it); });
-        XinvParams xp;
-        std::memcpy(xp.dvelgradavg, dvelgradavg, sizeof(xp.dvelgradavg));
-        if (inv3(dinvc, xp.dinv) != 0) throw SolveError("Singular matrix in lu_inverse (correction_to_current)", -3);
-        K("k_fft_x_inv", [&] { launch_fft_x_inv(d, pl1, 0, xp, st, prec_it); });
-        CorrParams cp;
-        cp.mix = mix;
-        cp.Lscale = std::max(lvmavg, EVP_TINY);
-        cp.do_mix = do_mix ? 1 : 0;
-        cp.kinematic = kinematic ? 1 : 0;
-        K("k_corr", [&] { launch_corr(d, cp, st); });
-        NewtonParams np;
-        np.tdot = p.tdot;
-        np.error = p.error;
-        np.erroral = p.erroral;
-        np.complgas = dk.complgas;
-        np.modal = modal ? 1 : 0;
-        np.thermo = (imicro == 1 && p.ithermo == 1) ? 1 : 0;
-        np.iuphard = p.iuphard;
-        K("k_newton", [&] { launch_newton(d, np, st); });
-        CK(cudaGetLastError());
-        fetch_red();
-        const double* cr = h_red + OFF_CORR;
-        for (int c = 0; c < 9; c++) {
-            velgradavg[c] = cr[c];
-            velgradavggas[c] = cr[9 + c];
-            velgradavgsol[c] = cr[18 + c];
+        did_converge = h_ctl->did_converge != 0;
+        accept_step = false;
+        if (ev == EV_CONVERGED) return true;
+        if (ev == EV_ACCEPTED) {
+            accept_step = true;
+            return true;
         }
-        if (wphcgas > 0.0)
-            for (int c = 0; c < 9; c++) velgradavggas[c] /= wphcgas;
-        for (int c = 0; c < 9; c++) velgradavgsol[c] /= wphcsol;
-        if (!kinematic) {
-            const double dls = cr[28] > 0.0 ? std::sqrt(cr[27] / cr[28]) : 0.0;
-            const double dlg = cr[30] > 0.0 ? std::sqrt(cr[29] / cr[30]) : 0.0;
-            const double dl = std::max(dls, dlg);
-            mix = std::max(1.0e-8, std::min(1.0, 5.0e-2 / std::max(dl, 5.0e-2)));
+        // EV_HOST: ictrl = -1 with tdot above tdotmin, at convergence or at ITMAX
+        bool restart = false;
+        double md;
+        if (!did_converge && iter == p.itmax) {
+            double tdot = p.tdot;
+            int nsub = kinematic_substep(tdot, md);
+            tdot = tdot / nsub;
+            tdot = std::max(p.tdotmin, std::min(tdot, 0.5 * p.tdot));
+            nsub = (int)std::ceil(p.tdot / tdot);
+            if (nsub > 1) {
+                const double remaining = std::max(0.0, proc_time_target - proc_time_done);
+                tdot_plan = tdot;
+                const int nnew = (imicro - 1) + (int)std::ceil(remaining / tdot_plan);
+                total_macrosteps += nnew - p.nsteps;
+                p.nsteps = nnew;
+                p.tdot = std::min(tdot_plan, remaining);
+                nconverged = 0;
+                restart = true;
+            }
+        } else if (did_converge) {
+            double tdot = p.tdot;
+            int nsub = kinematic_substep(tdot, md);
+            tdot = tdot / nsub;
+            if (md <= 1.0e-3) tdot = std::max(p.tdotmin, std::min(tdot, 0.5 * p.tdot));
+            else tdot = std::max(p.tdotmin, tdot);
+            nsub = (int)std::ceil(p.tdot / tdot);
+            if (nsub > 1) {
+                const double remaining = std::max(0.0, proc_time_target - proc_time_done);
+                tdot_plan = tdot;
+                const int nnew = (imicro - 1) + (int)std::ceil(remaining / tdot_plan);
+                total_macrosteps += nnew - p.nsteps;
+                p.nsteps = nnew;
+                p.tdot = std::min(tdot_plan, remaining);
+                did_converge = false;
+                nconverged = 0;
+                restart = true;
+            }
         }
-        const double* nw = h_red + OFF_NEWTON;
-        errs = nw[0];
-        erre = nw[1];
-        if (erre < 0 || errs < 0) throw SolveError("ERRE/ERRS negative -> convergence failed!", -4);
-        erre = std::sqrt(erre);
-        errs = std::sqrt(errs);
-        velgradavg_corr(nw + 2);
-        erre = erre / lvmavg;
-        errs = errs / svmavg;
-        errsbc = errsbc / svmavg;
+        if (iter >= 100000) throw SolveError("equilibrium iteration did not converge", -4);
+        if (restart) {  // roll the increment back and iterate it again with the cut time step
+            iter = 0;
+            snapshot(false);
+            start_iterations();
+            return false;
+        }
+        if (did_converge) return true;
+        resume_iterations();
+        return false;
     }
 
     int kinematic_substep(double tdot_step, double& min_detF) {
@@ -678,8 +720,13 @@ public:
         return std::max(1, (int)std::ceil(worst));
     }
 
-    // ------------------------------------------------------------ one macrostep (LS-EVPFFT.f90:199-588)
-    bool macrostep() {
+    // This solve as a member of a batched launch.
+    BatchSolve entry() const { return BatchSolve{d, pl1, pl2, pl3, d_ctl, d_c0, d_s0}; }
+
+    // ------------------------------------------------------------ increment start (LS-EVPFFT.f90:199-240)
+    // Process switch, time step, snapshot, form_G and the per-increment operators, then the
+    // control block of the first iteration.  False once the deck is finished.
+    bool begin_increment() {
         while (ipr == 0 || imicro >= P().nsteps) {
             if (ipr >= dk.nproc) { finished = true; return false; }
             ipr++;
@@ -698,7 +745,8 @@ public:
             p.tdot = (remaining > 0.0) ? std::min(tdot_plan, remaining) : tdot_plan;
         }
         snapshot(true);
-        bool did_converge = false, accept_step = false;
+        did_converge = false;
+        accept_step = false;
         const int do_schmid = ((imicro == 1 && ipr == 1) || p.iupdate == 1) ? 1 : 0;
         d.gtab = (p.igamma != 0 && d.goper) ? 1 : 0;
         if (d.gtab) K("k_goper_tab", [&] { launch_goper_tab(d, d_c0, d_s0, p.igamma, st); });  // form_G, IGAMMA 1, 2
@@ -710,88 +758,22 @@ public:
         }
         K("k_prologue", [&] { launch_prologue(d, d_c0, d_g0, do_schmid, modal ? 1 : 0, st); });
         iter = 0;
-        bool fresh = true;
-        while (!(did_converge || accept_step)) {
-            if (iter == 0) {
-                if (dk.has_gas) K("k_gas_compl", [&] { launch_gas_compl(d, p.tdot, dk.complgas, modal ? 1 : 0, st); });
-                std::memset(dvelgradavg, 0, sizeof(dvelgradavg));
-                edotvmmx = 0;
-                mix = 1.0;
-                erre = 2.0 * p.error; errs = 2.0 * p.error; errsbc = 2.0 * p.error;
-                fresh = true;
-                prec_it = prec;
-                err_hist.clear();
-            }
-            check_deadline();
-            iter++;
-            total_iters++;
-            if (verbose) {
-                std::printf("\rMACROSTEP=%d SimTime=%.0fs PROC=%d STEP=%d TDOT=%.0fs ITER=%d", imacroloop, sim_time, ipr, imicro, p.tdot, iter);
-                std::fflush(stdout);
-            }
-            equilibrium_iteration(fresh);
-            fresh = false;
-            if (p.ictrl == 0) {
-                double vs[9];
-                sym33(velgradavg, vs);
-                p.tdot = p.devmapp / vm_strain(vs);
-                p.tdotref = p.tdot;
-            }
-            if (errs <= p.error && erre <= p.error && errsbc <= p.error) did_converge = true;
-            if (prec_it != 0 && !did_converge) {  // FP32 stagnating above the tolerance: FP64 from here on
-                err_hist.push_back(std::max(errs, std::max(erre, errsbc)));
-                const size_t h = err_hist.size();
-                if (h >= 4 && err_hist[h - 1] > 0.7 * err_hist[h - 4]) prec_it = 0;
-            }
-            if (p.ictrl == -1) {
-                if (p.tdot > p.tdotmin) {
-                    double md;
-                    if (!did_converge && iter == p.itmax) {
-                        double tdot = p.tdot;
-                        int nsub = kinematic_substep(tdot, md);
-                        tdot = tdot / nsub;
-                        tdot = std::max(p.tdotmin, std::min(tdot, 0.5 * p.tdot));
-                        nsub = (int)std::ceil(p.tdot / tdot);
-                        if (nsub > 1) {
-                            const double remaining = std::max(0.0, proc_time_target - proc_time_done);
-                            tdot_plan = tdot;
-                            const int nnew = (imicro - 1) + (int)std::ceil(remaining / tdot_plan);
-                            total_macrosteps += nnew - p.nsteps;
-                            p.nsteps = nnew;
-                            p.tdot = std::min(tdot_plan, remaining);
-                            nconverged = 0;
-                            iter = 0;
-                            snapshot(false);
-                        }
-                    } else if (did_converge) {
-                        double tdot = p.tdot;
-                        int nsub = kinematic_substep(tdot, md);
-                        tdot = tdot / nsub;
-                        if (md <= 1.0e-3) tdot = std::max(p.tdotmin, std::min(tdot, 0.5 * p.tdot));
-                        else tdot = std::max(p.tdotmin, tdot);
-                        nsub = (int)std::ceil(p.tdot / tdot);
-                        if (nsub > 1) {
-                            const double remaining = std::max(0.0, proc_time_target - proc_time_done);
-                            tdot_plan = tdot;
-                            const int nnew = (imicro - 1) + (int)std::ceil(remaining / tdot_plan);
-                            total_macrosteps += nnew - p.nsteps;
-                            p.nsteps = nnew;
-                            p.tdot = std::min(tdot_plan, remaining);
-                            did_converge = false;
-                            nconverged = 0;
-                            iter = 0;
-                            mix = 1.0;
-                            snapshot(false);
-                        }
-                    }
-                } else if (iter == p.itmax) {
-                    accept_step = true;
-                }
-            }
-            if (iter >= 100000) throw SolveError("equilibrium iteration did not converge", -4);
-        }
-        const int iter_done = iter;
-        // commit + large-strain updates (LS-EVPFFT.f90:432-458)
+        start_iterations();
+        return true;
+    }
+
+    // ------------------------------------------------------------ increment end (LS-EVPFFT.f90:432-588)
+    // end_launch queues the commit, large-strain, diagnostics and calc_c0 kernels and the copy
+    // of their sums; end_finish, after the stream has been synchronised, does the host tails
+    // and writes the rows.  A batch launches the ends of many solves before one synchronisation.
+    struct EndState {
+        int iter_done = 0, nsteps_written = 0;
+        double tdot_used = 0, tdotref_used = 0;
+        bool conv_for_count = false;
+    } es;
+    void end_launch() {
+        ProcessData& p = P();
+        es.iter_done = iter;
         if (p.iupdate == 1) {  // update_grid_velgrad_node reads L and F before update_defgrad changes F
             K("k_grid_fft", [&] {
                 launch_fft_x_fwd(d, pl1, 1, 0, st);
@@ -827,16 +809,16 @@ public:
         const double Lref = std::max(lvmavg, EVP_TINY);
         K("k_diag", [&] { launch_diag(d, std::max(1.0e-12 * Lref, EVP_TINY), st); });
         // time bookkeeping and the tdot ramp are host-only; they fix the tdot calc_c0 sees.  The
-        // VTK "last step" test below uses the step count from before the ramp, as the reference
+        // VTK "last step" test uses the step count from before the ramp, as the reference
         // writes its fields before ramping (LS-EVPFFT.f90:525-535, then 557-581).
-        const int nsteps_written = p.nsteps;
-        const double tdot_used = p.tdot;
-        const double tdotref_used = p.tdotref;
+        es.nsteps_written = p.nsteps;
+        es.tdot_used = p.tdot;
+        es.tdotref_used = p.tdotref;
         if (p.ictrl == -1) {
-            proc_time_done += tdot_used;
+            proc_time_done += es.tdot_used;
             p.tdot = tdot_plan;
         }
-        sim_time += tdot_used;
+        sim_time += es.tdot_used;
         if (p.ictrl == -1) {
             if (tdot_plan < p.tdotref && nconverged >= 5) {
                 nconverged = 0;
@@ -857,11 +839,16 @@ public:
             total_macrosteps += left - (p.nsteps - imicro);
             p.nsteps = imicro + left;
         }
-        const bool conv_for_count = did_converge;
+        es.conv_for_count = did_converge;
         K("k_c0", [&] { launch_c0(d, p.tdot, p.tdotref, st); });
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev1, st));
-        fetch_red();
+        fetch_red_async();
+    }
+
+    void end_finish() {
+        check_red();
+        ProcessData& p = P();
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) gpu_ms += ms;
         // update_defgrad averages (host side of various_functions.f90:2250-2266)
@@ -896,22 +883,54 @@ public:
         dvmpavg = vm_strain(edotpavg);
         if (p.iwfields == 1) {
             const int aw = std::abs(p.iwstep);
-            const bool due = (aw != 0 && imicro % aw == 0) || (p.iwstep < 0 && imicro == nsteps_written);
+            const bool due = (aw != 0 && imicro % aw == 0) || (p.iwstep < 0 && imicro == es.nsteps_written);
             if (due && write_vtk_files) write_vtk(imacroloop);
         }
         finish_diag();
         dg.erre = erre; dg.errs = errs; dg.errsbc = errsbc;
-        dg.tdotref = tdotref_used;
+        dg.tdotref = es.tdotref_used;
         dg.s33_target = p.scauchy[8];
         dg.s33 = sgavg[8];
         dg.s33_sol = sgsolavg[8];
-        dg.devm_inc_max = edotvmmx * tdot_used;
+        dg.devm_inc_max = edotvmmx * es.tdot_used;
         wall_time = (double)(std::time(nullptr) - start);
-        write_rows(iter_done, imacroloop, ipr, sim_time, wall_time, tdot_used, dg.tdotref, gammaavg, gavg, geffavg);
-        if (conv_for_count) nconverged++;
+        write_rows(es.iter_done, imacroloop, ipr, sim_time, wall_time, es.tdot_used, dg.tdotref, gammaavg, gavg, geffavg);
+        if (es.conv_for_count) nconverged++;
         finish_c0(p);
         imacroloop++;
         macrosteps_done++;
+    }
+
+    // ------------------------------------------------------------ one macrostep of a solve on its own
+    // The engine of one member runs the increment's iterations; the host looks at the control
+    // block every check_every iterations (and at events: convergence, ITMAX, errors).
+    std::unique_ptr<Engine> solo;
+    int check_every = 4;
+    bool macrostep() {
+        if (!begin_increment()) return false;
+        if (!solo) {
+            solo.reset(new Engine(st));
+            solo->set_members({Engine::Member{entry(), modal ? 1 : 0, prec}});
+        } else {
+            solo->update_entry(0, entry());
+        }
+        Engine::Timer timer = [this](const char* name, const std::function<void()>& f) { K(name, f); };
+        const int per_iter = solo->launches_per_iteration();
+        long long rounds = 0;
+        while (true) {
+            check_deadline();
+            if (++rounds > 100000 / check_every + 100) throw SolveError("equilibrium iteration did not converge", -4);
+            solo->launch(check_every, profile ? &timer : nullptr);
+            if (!profile) launches += (long long)check_every * per_iter;
+            const int ev = solo->read_events()[0];
+            if (ev == EV_RUNNING) continue;
+            pull_ctl();
+            if (handle_event(ev)) break;
+            solo->update_entry(0, entry());
+        }
+        end_launch();
+        sync();
+        end_finish();
         return true;
     }
 
