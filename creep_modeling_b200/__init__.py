@@ -3,7 +3,7 @@
 The compute path is the sm_100a library ``_build/libevp_b200.so`` (C ABI in
 ``include/evp.h``); this package is the thin Python host over it.
 """
-from .solver import Solve, run_solver, load_results, RESULTS_COLS, DIAG_COLS  # noqa: F401
+from .solver import Batch, Solve, run_solver, solve_files, load_results, RESULTS_COLS, DIAG_COLS  # noqa: F401
 from ._lib import EvpError  # noqa: F401
 
-__all__ = ["Solve", "run_solver", "load_results", "RESULTS_COLS", "DIAG_COLS", "EvpError"]
+__all__ = ["Batch", "Solve", "run_solver", "solve_files", "load_results", "RESULTS_COLS", "DIAG_COLS", "EvpError"]

@@ -14,6 +14,7 @@ EXPORTED = (
     "evp_kernel_times", "evp_green_apply", "evp_green_apply_noalloc", "evp_last_error", "evp_version",
     "evp_server_open", "evp_submit", "evp_submit_deadline", "evp_poll", "evp_wait", "evp_server_close",
     "evp_set_deadline", "evp_kernel_launches", "evp_newton_stats",
+    "evp_batch_open", "evp_batch_add", "evp_batch_step", "evp_batch_status", "evp_batch_close", "evp_solve_files",
 )
 
 STATUS = {
@@ -99,6 +100,20 @@ def load(path: Path | str | None = None):
     L.evp_kernel_times.restype = ctypes.c_int
     L.evp_newton_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.evp_newton_stats.restype = ctypes.c_int
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.evp_batch_open.argtypes = [ctypes.POINTER(vp)]
+    L.evp_batch_open.restype = ctypes.c_int
+    L.evp_batch_add.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip]
+    L.evp_batch_add.restype = ctypes.c_int
+    L.evp_batch_step.argtypes = [vp, ctypes.c_int, ip]
+    L.evp_batch_step.restype = ctypes.c_int
+    L.evp_batch_status.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(Report), ctypes.c_char_p, ctypes.c_int]
+    L.evp_batch_status.restype = ctypes.c_int
+    L.evp_batch_close.argtypes = [vp]
+    L.evp_batch_close.restype = ctypes.c_int
+    L.evp_solve_files.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_char_p),
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Report)]
+    L.evp_solve_files.restype = ctypes.c_int
     L.evp_kernel_launches.argtypes = [vp]
     L.evp_kernel_launches.restype = ctypes.c_longlong
     L.evp_green_apply.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, vp]

@@ -187,6 +187,16 @@ struct BatchLaunch {
     int blocks, threads;
     size_t smem;
 };
+// The members of one batched launch travel as its kernel parameter (a __grid_constant__
+// struct in the constant bank: read-only and uniform, so the bodies' loads of sizes and
+// pointers are as cheap as a single-solve launch's).  Up to kBatchChunk members per launch
+// (26.6 kB of the 32 kB parameter space); larger batches take several launches per pass.
+constexpr int kBatchChunk = 40;
+struct BatchParams {
+    int njobs, pad;
+    Job jobs[kBatchChunk];  // job.solve indexes E
+    BatchSolve E[kBatchChunk];
+};
 // Job-table entries of one member for every pass it takes part in (host side of the batch
 // plan): [0] the FP64 launch shape of each pass, [1] the FP32 one of the spectral passes of a
 // mixed-precision member (has32).
@@ -199,23 +209,17 @@ struct MemberJobs {
 };
 
 #ifdef __CUDACC__
-// Block side of a batched launch: the member whose job covers this block (binary search on
-// blk0), the member's descriptor copied to shared memory, and the solve-local block.
-static_assert(sizeof(BatchSolve) % 8 == 0, "BatchSolve is copied in 8-byte words");
-__device__ __forceinline__ Job batch_job(const Job* __restrict__ jobs, int njobs) {
-    int lo = 0, hi = njobs - 1;
+// Block side of a batched launch: the job (member) covering this block (binary search on
+// blk0) and the solve-local block coordinates inside it.
+__device__ __forceinline__ const Job& batch_job(const BatchParams& P) {
+    int lo = 0, hi = P.njobs - 1;
     const int b = blockIdx.x;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (jobs[mid].blk0 <= b) lo = mid;
+        if (P.jobs[mid].blk0 <= b) lo = mid;
         else hi = mid - 1;
     }
-    return jobs[lo];
-}
-__device__ __forceinline__ void load_member(BatchSolve& dst, const BatchSolve* __restrict__ src) {
-    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(src);
-    unsigned long long* b = reinterpret_cast<unsigned long long*>(&dst);
-    for (int i = threadIdx.x; i < (int)(sizeof(BatchSolve) / 8); i += blockDim.x) b[i] = a[i];
+    return P.jobs[lo];
 }
 __device__ __forceinline__ VB job_vb(const Job& jb) {
     const int l = (int)blockIdx.x - jb.blk0;
@@ -251,8 +255,8 @@ void launch_cell2node(const Dev& d, double tdot, int ideriv, cudaStream_t st);
 // and tile) and the launches over a job table (E, jobs: device arrays).
 void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj);
 void member_jobs_fft(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, int prec, MemberJobs& mj);
-void launch_batched_voxel(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st);
-void launch_batched_fft(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st);
+void launch_batched_voxel(const BatchLaunch& L, const BatchParams& P, cudaStream_t st);
+void launch_batched_fft(const BatchLaunch& L, const BatchParams& P, cudaStream_t st);
 // the serial tail of one iteration for n solves (evp_control.cu); events[i] = EV_* or a status code
 void launch_control(const BatchSolve* E, int n, int* events, cudaStream_t st);
 

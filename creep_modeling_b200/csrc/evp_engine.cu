@@ -45,7 +45,6 @@ static bool fft_kind(int k) { return k == BK_XFWD || k == BK_YFWD || k == BK_ZGR
 Engine::~Engine() {
     drop_graph();
     if (dE_) cudaFreeAsync(dE_, st_);
-    if (dJobs_) cudaFreeAsync(dJobs_, st_);
     if (dEv_) cudaFreeAsync(dEv_, st_);
     if (hEv_) cudaFreeHost(hEv_);
 }
@@ -77,9 +76,9 @@ void Engine::set_members(const std::vector<Member>& m) {
         member_jobs_voxel(m[i].e.d, m[i].modal, mj[i]);
         member_jobs_fft(m[i].e.d, m[i].e.pl1, m[i].e.pl2, m[i].e.pl3, m[i].prec, mj[i]);
     }
-    // one launch per pass, spectral precision and kernel variant, members in membership order
-    std::vector<BatchLaunch> plan;
-    std::vector<Job> jobs;
+    // one launch per pass, spectral precision and kernel variant (and per kBatchChunk members),
+    // members in membership order
+    plan_.clear();
     for (int k = 0; k < BK_N; k++) {
         for (int w = 0; w < (fft_kind(k) ? 2 : 1); w++) {
             std::map<int, std::vector<int>> byvar;
@@ -88,55 +87,64 @@ void Engine::set_members(const std::vector<Member>& m) {
                 byvar[mj[i].variant[w][k]].push_back(i);
             }
             for (auto& kv : byvar) {
-                BatchLaunch L{};
-                L.kind = k;
-                L.variant = kv.first;
-                L.job0 = (int)jobs.size();
-                L.njobs = (int)kv.second.size();
-                long long blocks = 0;
-                for (int i : kv.second) {
-                    Job j = mj[i].job[w][k];
-                    j.solve = i;
-                    j.blk0 = (int)blocks;
-                    blocks += (long long)j.gx * j.gy * j.gz;
-                    L.threads = std::max(L.threads, mj[i].threads[w][k]);
-                    L.smem = std::max(L.smem, mj[i].smem[w][k]);
-                    jobs.push_back(j);
+                for (size_t c0 = 0; c0 < kv.second.size(); c0 += kBatchChunk) {
+                    plan_.emplace_back();
+                    Launch& ln = plan_.back();
+                    std::memset(&ln.P, 0, sizeof(BatchParams));
+                    ln.L = BatchLaunch{};
+                    ln.L.kind = k;
+                    ln.L.variant = kv.first;
+                    long long blocks = 0;
+                    for (size_t c = c0; c < std::min(kv.second.size(), c0 + (size_t)kBatchChunk); c++) {
+                        const int i = kv.second[c];
+                        const int q = ln.P.njobs++;
+                        Job j = mj[i].job[w][k];
+                        j.solve = q;
+                        j.blk0 = (int)blocks;
+                        blocks += (long long)j.gx * j.gy * j.gz;
+                        ln.P.jobs[q] = j;
+                        ln.P.E[q] = m[i].e;
+                        ln.members.push_back(i);
+                        ln.L.threads = std::max(ln.L.threads, mj[i].threads[w][k]);
+                        ln.L.smem = std::max(ln.L.smem, mj[i].smem[w][k]);
+                    }
+                    if (blocks >= (1LL << 31)) throw SolveError("batched launch larger than the grid limit", -7);
+                    ln.L.blocks = (int)blocks;
+                    ln.L.njobs = ln.P.njobs;
                 }
-                if (blocks >= (1LL << 31)) throw SolveError("batched launch larger than the grid limit", -7);
-                L.blocks = (int)blocks;
-                plan.push_back(L);
             }
         }
     }
-    plan_ = plan;
     drop_graph();
     if (n == 0) return;
     dE_ = grow(dE_, capE_, (size_t)n);
-    dJobs_ = grow(dJobs_, capJobs_, jobs.size());
     dEv_ = grow(dEv_, capEv_, (size_t)n);
     std::vector<BatchSolve> E(n);
     for (int i = 0; i < n; i++) E[i] = m[i].e;
     ECK(cudaMemcpyAsync(dE_, E.data(), n * sizeof(BatchSolve), cudaMemcpyHostToDevice, st_));
-    ECK(cudaMemcpyAsync(dJobs_, jobs.data(), jobs.size() * sizeof(Job), cudaMemcpyHostToDevice, st_));
     if (hEv_) cudaFreeHost(hEv_);
     hEv_ = nullptr;
     ECK(cudaMallocHost(&hEv_, n * sizeof(int)));
 }
 
 void Engine::update_entry(int i, const BatchSolve& e) {
+    if (std::memcmp(&members_[i].e, &e, sizeof(BatchSolve)) == 0) return;
     members_[i].e = e;
+    for (Launch& ln : plan_)
+        for (size_t q = 0; q < ln.members.size(); q++)
+            if (ln.members[q] == i) ln.P.E[q] = e;
     ECK(cudaMemcpyAsync(dE_ + i, &members_[i].e, sizeof(BatchSolve), cudaMemcpyHostToDevice, st_));
+    drop_graph();  // the captured launches carry the old descriptor
 }
 
 void Engine::launch_one_iteration(const Timer* timer) {
-    for (const BatchLaunch& L : plan_) {
-        if (L.blocks == 0) continue;
+    for (const Launch& ln : plan_) {
+        if (ln.L.blocks == 0) continue;
         auto f = [&] {
-            if (fft_kind(L.kind)) launch_batched_fft(L, dE_, dJobs_, st_);
-            else launch_batched_voxel(L, dE_, dJobs_, st_);
+            if (fft_kind(ln.L.kind)) launch_batched_fft(ln.L, ln.P, st_);
+            else launch_batched_voxel(ln.L, ln.P, st_);
         };
-        if (timer) (*timer)(kind_name(L.kind), f);
+        if (timer) (*timer)(kind_name(ln.L.kind), f);
         else f();
     }
     auto c = [&] { launch_control(dE_, (int)members_.size(), dEv_, st_); };

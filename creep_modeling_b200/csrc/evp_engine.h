@@ -67,14 +67,18 @@ private:
     template <class T>
     T* grow(T* p, size_t& cap, size_t n);
 
+    struct Launch {
+        BatchLaunch L;
+        BatchParams P;             // the launch's members (kernel parameter)
+        std::vector<int> members;  // their indices in the membership
+    };
     cudaStream_t st_;
     std::vector<Member> members_;
-    std::vector<BatchLaunch> plan_;
-    BatchSolve* dE_ = nullptr;
-    Job* dJobs_ = nullptr;
+    std::vector<Launch> plan_;
+    BatchSolve* dE_ = nullptr;  // every member's descriptor, for k_control
     int* dEv_ = nullptr;
     int* hEv_ = nullptr;
-    size_t capE_ = 0, capJobs_ = 0, capEv_ = 0;
+    size_t capE_ = 0, capEv_ = 0;
     cudaGraphExec_t graph_ = nullptr;
     int graph_k_ = 0;
 };

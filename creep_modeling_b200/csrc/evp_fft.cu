@@ -990,8 +990,8 @@ void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvPar
 }
 
 // ---------------------------------------------------------------- batched launches of the iteration's spectral passes
-// As the voxel passes (evp_kernels.cu): each block finds its member, copies the member's
-// descriptor to shared memory and runs the member's body on its own block coordinates.
+// As the voxel passes (evp_kernels.cu): each block finds its member in the launch's
+// parameter and runs the member's body on its own block coordinates.
 // A member takes part in the FP64 launch of a pass while its control block asks for FP64
 // spectra and in the FP32 launch while it asks for FP32 (mixed precision).
 template <class CT>
@@ -999,53 +999,35 @@ __device__ __forceinline__ bool batch_go(const IterCtl* c) {
     return c->active && ((c->prec != 0) == (sizeof(CT) == sizeof(float2)));
 }
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, 2) kb_fft_x_fwd(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
-    __shared__ int go, sg_off;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
-    if (threadIdx.x == 0) {
-        const IterCtl* c = E[jb.solve].ctl;
-        go = batch_go<CT>(c);
-        sg_off = c->sg_off;
-    }
-    __syncthreads();
-    if (!go) return;
-    body_fft_x_fwd<RS, CT>(m.d, m.pl1, jb.tile, 0, sg_off, job_vb(jb));
+__global__ void __launch_bounds__(256, 2) kb_fft_x_fwd(const __grid_constant__ BatchParams P) {
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
+    if (!batch_go<CT>(m.ctl)) return;
+    body_fft_x_fwd<RS, CT>(m.d, m.pl1, jb.tile, 0, m.ctl->sg_off, job_vb(jb));
 }
 template <bool INV, int RS, class CT>
-__global__ void __launch_bounds__(256, 2) kb_fft_y(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
-    __shared__ int go;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
-    if (threadIdx.x == 0) go = batch_go<CT>(E[jb.solve].ctl);
-    __syncthreads();
-    if (!go) return;
+__global__ void __launch_bounds__(256, 2) kb_fft_y(const __grid_constant__ BatchParams P) {
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
+    if (!batch_go<CT>(m.ctl)) return;
     body_fft_y<INV, RS, CT>(m.d, m.pl2, jb.tile, job_vb(jb));
 }
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, 2) kb_fft_z_green(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
-    __shared__ int go;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
-    if (threadIdx.x == 0) go = batch_go<CT>(E[jb.solve].ctl);
-    __syncthreads();
-    if (!go) return;
+__global__ void __launch_bounds__(256, 2) kb_fft_z_green(const __grid_constant__ BatchParams P) {
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
+    if (!batch_go<CT>(m.ctl)) return;
     body_fft_z_green<RS, CT>(m.d, m.pl3, jb.tile, m.c0, m.s0, job_vb(jb));
 }
 template <int RS, class CT>
-__global__ void __launch_bounds__(256, 2) kb_fft_x_inv(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
+__global__ void __launch_bounds__(256, 2) kb_fft_x_inv(const __grid_constant__ BatchParams P) {
     __shared__ XinvParams xp;
     __shared__ int go;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
     if (threadIdx.x == 0) {
-        const IterCtl* c = E[jb.solve].ctl;
-        go = batch_go<CT>(c);
-        xp = c->xinv;
+        go = batch_go<CT>(m.ctl);
+        xp = m.ctl->xinv;
     }
     __syncthreads();
     if (!go) return;
@@ -1078,23 +1060,22 @@ void member_jobs_fft(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, c
 }
 
 template <int RS, class CT>
-static void batched_fft_ct(const BatchLaunch& L, const BatchSolve* E, const Job* J, cudaStream_t st) {
+static void batched_fft_ct(const BatchLaunch& L, const BatchParams& P, cudaStream_t st) {
     switch (L.kind) {
-        case BK_XFWD: kb_fft_x_fwd<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-        case BK_YFWD: kb_fft_y<false, RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-        case BK_ZGREEN: kb_fft_z_green<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-        case BK_YINV: kb_fft_y<true, RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-        case BK_XINV: kb_fft_x_inv<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+        case BK_XFWD: kb_fft_x_fwd<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+        case BK_YFWD: kb_fft_y<false, RS, CT><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+        case BK_ZGREEN: kb_fft_z_green<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+        case BK_YINV: kb_fft_y<true, RS, CT><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+        case BK_XINV: kb_fft_x_inv<RS, CT><<<L.blocks, L.threads, L.smem, st>>>(P); break;
         default: break;
     }
 }
-void launch_batched_fft(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st) {
-    const Job* J = jobs + L.job0;
+void launch_batched_fft(const BatchLaunch& L, const BatchParams& P, cudaStream_t st) {
     switch (L.variant) {
-        case 0: batched_fft_ct<0, double2>(L, E, J, st); break;
-        case 1: batched_fft_ct<1, double2>(L, E, J, st); break;
-        case 2: batched_fft_ct<0, float2>(L, E, J, st); break;
-        default: batched_fft_ct<1, float2>(L, E, J, st); break;
+        case 0: batched_fft_ct<0, double2>(L, P, st); break;
+        case 1: batched_fft_ct<1, double2>(L, P, st); break;
+        case 2: batched_fft_ct<0, float2>(L, P, st); break;
+        default: batched_fft_ct<1, float2>(L, P, st); break;
     }
 }
 

@@ -1776,8 +1776,7 @@ static size_t newton_smem(const Dev& d, int variant) {
     }
 }
 template <int V>
-__global__ void __launch_bounds__(V >= 6 ? 128 : 256, 2) kb_newton(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs,
-                                                                   int njobs);
+__global__ void __launch_bounds__(V >= 6 ? 128 : 256, 2) kb_newton(const __grid_constant__ BatchParams P);
 static void newton_configure() {
     static std::once_flag once;
     std::call_once(once, [] {
@@ -1813,52 +1812,42 @@ void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------- batched launches of the iteration's voxel passes
-// Each block finds its member in the job table (binary search on blk0), copies the
-// member's descriptor to shared memory, reads its control block and runs the same
-// body as the member's single-solve launch, on the member's own block coordinates.
-// Blocks of members that are not iterating (converged, waiting for the host) exit.
-__global__ void __launch_bounds__(kBlock) kb_sgavg(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
-    __shared__ int go;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
-    if (threadIdx.x == 0) {
-        const IterCtl* c = E[jb.solve].ctl;
-        go = c->active && c->fresh;
-    }
-    __syncthreads();
-    if (!go) return;
+// Each block finds its member in the launch's parameter (binary search on blk0), reads
+// the member's control block and runs the same body as the member's single-solve
+// launch, on the member's own block coordinates.  Blocks of members that are not
+// iterating (converged, waiting for the host) exit at once.
+__global__ void __launch_bounds__(kBlock) kb_sgavg(const __grid_constant__ BatchParams P) {
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
+    if (!(m.ctl->active && m.ctl->fresh)) return;  // uniform over the block
     body_sgavg(m.d, job_vb(jb));
 }
-__global__ void __launch_bounds__(kBlock, 2) kb_corr(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
+__global__ void __launch_bounds__(kBlock, 2) kb_corr(const __grid_constant__ BatchParams P) {
     __shared__ CorrParams p;
     __shared__ int go;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
     if (threadIdx.x == 0) {
-        const IterCtl* c = E[jb.solve].ctl;
-        go = c->active;
-        p = c->corr;
+        go = m.ctl->active;
+        p = m.ctl->corr;
     }
     __syncthreads();
     if (!go) return;
     body_corr(m.d, p, job_vb(jb));
 }
 template <int V>
-__global__ void __launch_bounds__(V >= 6 ? kNewtonBlock : 256, 2) kb_newton(const BatchSolve* __restrict__ E, const Job* __restrict__ jobs, int njobs) {
-    __shared__ BatchSolve m;
-    __shared__ NewtonParams p;
+__global__ void __launch_bounds__(V >= 6 ? 128 : 256, 2) kb_newton(const __grid_constant__ BatchParams P) {
+    __shared__ NewtonParams ps;
     __shared__ int go;
-    const Job jb = batch_job(jobs, njobs);
-    load_member(m, E + jb.solve);
+    const Job& jb = batch_job(P);
+    const BatchSolve& m = P.E[jb.solve];
     if (threadIdx.x == 0) {
-        const IterCtl* c = E[jb.solve].ctl;
-        go = c->active;
-        p = c->newton;
+        go = m.ctl->active;
+        ps = m.ctl->newton;
     }
     __syncthreads();
     if (!go) return;
+    const NewtonParams p = ps;  // in registers, as a single-solve launch's parameter
     const VB vb = job_vb(jb);
     if constexpr (V == 0) body_newton6p<2>(m.d, p, vb);
     else if constexpr (V == 1) body_newton6p<4>(m.d, p, vb);
@@ -1869,6 +1858,7 @@ __global__ void __launch_bounds__(V >= 6 ? kNewtonBlock : 256, 2) kb_newton(cons
     else if constexpr (V == 6) body_newton1<12>(m.d, p, vb);
     else body_newton1<24>(m.d, p, vb);
 }
+
 void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj) {
     newton_configure();
     auto one_d = [&](int k, int grid, int thr, size_t sm, int variant) {
@@ -1883,21 +1873,20 @@ void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj) {
     one_d(BK_NEWTON, newton_grid(d, v), v >= 6 ? kNewtonBlock : 256, newton_smem(d, v), v);
 }
 
-void launch_batched_voxel(const BatchLaunch& L, const BatchSolve* E, const Job* jobs, cudaStream_t st) {
-    const Job* J = jobs + L.job0;
+void launch_batched_voxel(const BatchLaunch& L, const BatchParams& P, cudaStream_t st) {
     switch (L.kind) {
-        case BK_SGAVG: kb_sgavg<<<L.blocks, L.threads, 0, st>>>(E, J, L.njobs); break;
-        case BK_CORR: kb_corr<<<L.blocks, L.threads, 0, st>>>(E, J, L.njobs); break;
+        case BK_SGAVG: kb_sgavg<<<L.blocks, L.threads, 0, st>>>(P); break;
+        case BK_CORR: kb_corr<<<L.blocks, L.threads, 0, st>>>(P); break;
         case BK_NEWTON:
             switch (L.variant) {
-                case 0: kb_newton<0><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                case 1: kb_newton<1><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                case 2: kb_newton<2><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                case 3: kb_newton<3><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                case 4: kb_newton<4><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                case 5: kb_newton<5><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                case 6: kb_newton<6><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
-                default: kb_newton<7><<<L.blocks, L.threads, L.smem, st>>>(E, J, L.njobs); break;
+                case 0: kb_newton<0><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                case 1: kb_newton<1><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                case 2: kb_newton<2><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                case 3: kb_newton<3><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                case 4: kb_newton<4><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                case 5: kb_newton<5><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                case 6: kb_newton<6><<<L.blocks, L.threads, L.smem, st>>>(P); break;
+                default: kb_newton<7><<<L.blocks, L.threads, L.smem, st>>>(P); break;
             }
             break;
         default: break;

@@ -8,6 +8,7 @@
 // calc_c0, convergence and time-step control) run on those sums in FP64.
 #include "../../include/evp.h"
 #include "evp_deck.h"
+#include "evp_batch.h"
 #include "evp_dev.cuh"
 #include "evp_engine.h"
 #include "evp_math.cuh"
@@ -244,8 +245,10 @@ public:
     // back-to-back solves reuse the memory.
 
     // ------------------------------------------------------------ open (LS-EVPFFT.f90:144-178)
+    // ext_stream: run on the caller's stream (a batch's); parsed: the deck, already read (the
+    // server parses decks on the submitting thread)
     void open(const std::string& fft_in, const std::string& out, int mix_flag, int modal_flag, int flags,
-              cudaStream_t ext_stream = nullptr) {
+              cudaStream_t ext_stream = nullptr, Deck* parsed = nullptr) {
         write_files = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV)) != 0;
         write_vtk_files = (flags & EVP_WRITE_FILES) != 0;
         profile = (flags & EVP_PROFILE) != 0;
@@ -263,10 +266,14 @@ public:
                 if ((ext == ".vtk" || ext == ".out") && e.is_regular_file(ec2)) std::filesystem::remove(e.path(), ec2);
             }
         }
-        try {
-            dk = parse_deck(fft_in);
-        } catch (DeckError& e) {
-            throw SolveError(e.what(), e.code);
+        if (parsed) {
+            dk = std::move(*parsed);
+        } else {
+            try {
+                dk = parse_deck(fft_in);
+            } catch (DeckError& e) {
+                throw SolveError(e.what(), e.code);
+            }
         }
         int dev_count = 0;
         if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) throw SolveError("no CUDA device available", -6);
@@ -1246,6 +1253,197 @@ public:
     }
 };
 
+// ------------------------------------------------------------ a batch of solves (evp_batch.h)
+class Batch {
+public:
+    struct Slot {
+        std::unique_ptr<Solver> s;
+        int state = 0;  // 0 running, 1 finished
+        int status = 0;
+        std::string err;
+        evp_report rep{};
+        std::chrono::steady_clock::time_point t0;
+    };
+    cudaStream_t st = nullptr;
+    std::unique_ptr<Engine> eng;
+    std::vector<Slot> slots;  // slot ids stay valid; a removed slot keeps its record, not its solver
+    std::vector<int> members;  // running slots, in the engine's member order
+    bool dirty = false;
+    int check_every = 4;
+
+    Batch() {
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        eng.reset(new Engine(st));
+    }
+    ~Batch() {
+        eng.reset();
+        for (auto& sl : slots) sl.s.reset();
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    }
+
+    void finish(int id, int status, const std::string& err) {
+        Slot& sl = slots[id];
+        if (sl.state == 1) return;
+        sl.state = 1;
+        sl.status = status;
+        sl.err = err;
+        std::memset(&sl.rep, 0, sizeof(sl.rep));
+        if (sl.s) {
+            Solver& s = *sl.s;
+            sl.rep.macrosteps = s.macrosteps_done;
+            sl.rep.equilibrium_iters = s.total_iters;
+            sl.rep.voxel_iters = s.total_iters * s.d.N;
+            sl.rep.n1 = s.d.n1;
+            sl.rep.n2 = s.d.n2;
+            sl.rep.n3 = s.d.n3;
+            sl.rep.h2d_bytes = s.h2d;
+            sl.rep.d2h_bytes = s.d2h;
+        }
+        sl.rep.status = status;
+        sl.rep.wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - sl.t0).count();
+        dirty = true;
+    }
+
+    int add(Deck&& dk, const std::string& fft_in, const std::string& out, int mix, int modal, int flags, double deadline_s,
+            std::string& err) {
+        const int id = (int)slots.size();
+        slots.emplace_back();
+        slots[id].t0 = std::chrono::steady_clock::now();
+        slots[id].s.reset(new Solver());
+        Solver& s = *slots[id].s;
+        try {
+            s.open(fft_in, out, mix, modal, flags & ~EVP_PROFILE, st, &dk);
+            if (deadline_s > 0.0) {
+                s.has_deadline = true;
+                s.deadline = slots[id].t0 + std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                                                std::chrono::duration<double>(deadline_s));
+            }
+            if (!s.begin_increment()) {
+                finish(id, 0, "");
+                return id;
+            }
+        } catch (SolveError& e) {
+            err = e.what();
+            finish(id, e.code, err);
+            slots[id].s.reset();
+            return id;
+        } catch (std::exception& e) {
+            err = e.what();
+            finish(id, -1, err);
+            slots[id].s.reset();
+            return id;
+        }
+        dirty = true;
+        return id;
+    }
+
+    void rebuild() {
+        members.clear();
+        std::vector<Engine::Member> m;
+        for (int id = 0; id < (int)slots.size(); id++) {
+            if (slots[id].state != 0 || !slots[id].s) continue;
+            members.push_back(id);
+            Solver& s = *slots[id].s;
+            m.push_back(Engine::Member{s.entry(), s.modal ? 1 : 0, s.prec});
+        }
+        eng->set_members(m);
+        dirty = false;
+    }
+
+    // one round: check_every iterations of every running member, then the host side of their events
+    void round() {
+        if (dirty) rebuild();
+        if (members.empty()) return;
+        eng->launch(check_every, nullptr);
+        const int per_iter = eng->launches_per_iteration();
+        const int* ev = eng->read_events();
+        std::vector<int> ended;  // member positions whose increment iteration is over
+        for (int i = 0; i < (int)members.size(); i++) {
+            const int id = members[i];
+            Solver& s = *slots[id].s;
+            s.launches += (long long)check_every * per_iter;
+            try {
+                s.check_deadline();
+                if (ev[i] == EV_RUNNING) continue;
+                s.pull_ctl();
+                if (s.handle_event(ev[i])) ended.push_back(i);
+                else eng->update_entry(i, s.entry());
+            } catch (SolveError& e) {
+                finish(id, e.code, e.what());
+            } catch (std::exception& e) {
+                finish(id, -1, e.what());
+            }
+        }
+        std::vector<int> launched;
+        for (int i : ended) {
+            const int id = members[i];
+            if (slots[id].state != 0) continue;
+            try {
+                slots[id].s->end_launch();
+                launched.push_back(i);
+            } catch (SolveError& e) {
+                finish(id, e.code, e.what());
+            }
+        }
+        if (!launched.empty()) CK(cudaStreamSynchronize(st));
+        for (int i : launched) {
+            const int id = members[i];
+            Solver& s = *slots[id].s;
+            try {
+                s.end_finish();
+                if (!s.begin_increment()) finish(id, 0, "");
+                else eng->update_entry(i, s.entry());
+            } catch (SolveError& e) {
+                finish(id, e.code, e.what());
+            } catch (std::exception& e) {
+                finish(id, -1, e.what());
+            }
+        }
+    }
+
+    int running() const {
+        int n = 0;
+        for (auto& sl : slots) n += (sl.state == 0 && sl.s) ? 1 : 0;
+        return n;
+    }
+};
+
+Batch* batch_create() { return new Batch(); }
+void batch_destroy(Batch* b) { delete b; }
+int batch_add(Batch* b, Deck&& dk, const std::string& fft_in, const std::string& out_dir, int mix, int modal, int flags,
+              double deadline_s, std::string& err) {
+    return b->add(std::move(dk), fft_in, out_dir, mix, modal, flags, deadline_s, err);
+}
+int batch_step(Batch* b, int rounds) {
+    for (int r = 0; r < rounds; r++) {
+        b->round();
+        if (b->running() == 0) break;
+    }
+    if (b->dirty) b->rebuild();
+    return b->running();
+}
+int batch_slot(Batch* b, int slot, int* status, evp_report* rep, std::string* err) {
+    if (slot < 0 || slot >= (int)b->slots.size()) return -1;
+    const Batch::Slot& sl = b->slots[slot];
+    if (status) *status = sl.status;
+    if (rep) *rep = sl.rep;
+    if (err) *err = sl.err;
+    return sl.state;
+}
+void batch_remove(Batch* b, int slot) {
+    if (slot < 0 || slot >= (int)b->slots.size()) return;
+    Batch::Slot& sl = b->slots[slot];
+    if (sl.state == 0) {
+        b->finish(slot, -7, "removed while running");
+    }
+    sl.s.reset();
+    b->dirty = true;
+}
+int batch_running(Batch* b) { return b->running(); }
+
 }  // namespace evp
 
 using evp::SolveError;
@@ -1380,6 +1578,116 @@ int evp_newton_stats(evp_solve* h, long long* out6) {
 int evp_close(evp_solve* h) {
     delete h;
     return 0;
+}
+
+struct evp_batch {
+    evp::Batch* b = nullptr;
+};
+
+int evp_batch_open(evp_batch** out) {
+    if (!out) return fail("evp_batch_open: null argument", -7);
+    *out = nullptr;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return fail("no CUDA device available", -6);
+    try {
+        evp_batch* h = new evp_batch();
+        h->b = evp::batch_create();
+        *out = h;
+    } catch (SolveError& e) {
+        return fail(e.what(), e.code);
+    }
+    return 0;
+}
+
+int evp_batch_add(evp_batch* h, const char* fft_in, const char* out_dir, int mix, int modal, int flags, int* slot) {
+    if (!h || !fft_in || !slot) return fail("evp_batch_add: null argument", -7);
+    evp::Deck dk;
+    try {
+        dk = evp::parse_deck(fft_in);
+    } catch (evp::DeckError& e) {
+        return fail(e.what(), e.code);
+    } catch (std::exception& e) {
+        return fail(e.what(), -1);
+    }
+    std::string err;
+    try {
+        *slot = evp::batch_add(h->b, std::move(dk), fft_in, out_dir ? out_dir : "", mix, modal, flags, 0.0, err);
+    } catch (SolveError& e) {
+        return fail(e.what(), e.code);
+    }
+    int status = 0;
+    evp::batch_slot(h->b, *slot, &status, nullptr, nullptr);
+    if (status != 0) return fail(err, status);
+    return 0;
+}
+
+int evp_batch_step(evp_batch* h, int rounds, int* running) {
+    if (!h) return fail("evp_batch_step: null handle", -7);
+    try {
+        const int n = evp::batch_step(h->b, rounds > 0 ? rounds : 1);
+        if (running) *running = n;
+    } catch (SolveError& e) {
+        return fail(e.what(), e.code);
+    } catch (std::exception& e) {
+        return fail(e.what(), -1);
+    }
+    return 0;
+}
+
+int evp_batch_status(evp_batch* h, int slot, int* state, evp_report* rep, char* msg, int msgcap) {
+    if (!h) return fail("evp_batch_status: null handle", -7);
+    int status = 0;
+    std::string err;
+    const int s = evp::batch_slot(h->b, slot, &status, rep, &err);
+    if (s < 0) return fail("evp_batch_status: no such slot", -7);
+    if (state) *state = s;
+    if (msg && msgcap > 0) {
+        std::strncpy(msg, err.c_str(), (size_t)msgcap - 1);
+        msg[msgcap - 1] = '\0';
+    }
+    return 0;
+}
+
+int evp_batch_close(evp_batch* h) {
+    if (!h) return 0;
+    evp::batch_destroy(h->b);
+    delete h;
+    return 0;
+}
+
+int evp_solve_files(int n, const char* const* fft_in, const char* const* out_dir, int mix, int modal, int flags,
+                    evp_report* reports) {
+    if (n < 0 || (n > 0 && (!fft_in || !reports))) return fail("evp_solve_files: null argument", -7);
+    evp_batch* h = nullptr;
+    int rc = evp_batch_open(&h);
+    if (rc != 0) return rc;
+    std::vector<int> slots(n, -1);
+    int worst = 0;
+    for (int i = 0; i < n; i++) {
+        const int r = evp_batch_add(h, fft_in[i], out_dir ? out_dir[i] : "", mix, modal,
+                                    flags ? flags : EVP_WRITE_FILES, &slots[i]);
+        if (r != 0 && slots[i] < 0) {
+            std::memset(&reports[i], 0, sizeof(evp_report));
+            reports[i].status = r;
+            worst = worst ? worst : r;
+        }
+    }
+    int running = 1;
+    while (running > 0) {
+        rc = evp_batch_step(h, 16, &running);
+        if (rc != 0) {
+            evp_batch_close(h);
+            return rc;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        if (slots[i] < 0) continue;
+        int state = 0;
+        evp_batch_status(h, slots[i], &state, &reports[i], nullptr, 0);
+        if (reports[i].status != 0 && worst == 0) worst = reports[i].status;
+    }
+    evp_batch_close(h);
+    return worst;
 }
 
 int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const char* fftw_save, int mix, int modal, evp_report* report) {

@@ -139,3 +139,73 @@ class Solve:
 def load_results(path) -> np.ndarray:
     """results.csv as a float array (columns RESULTS_COLS)."""
     return np.loadtxt(Path(path), delimiter=",", skiprows=1, ndmin=2)
+
+
+class Batch:
+    """Many solves advanced together (``evp_batch_*`` of ``include/evp.h``): one launch per pass
+    of every equilibrium iteration over all running members, a device-side controller for each
+    member's serial tail, the iterations replayed as a CUDA graph.  Members start and finish
+    increments independently; each member's results equal those of its solve alone."""
+
+    def __init__(self):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(L.evp_batch_open(ctypes.byref(h)))
+        self._h = h
+
+    def add(self, fft_in, out_dir="", mix=1, modal=0, write_files=False, csv_only=True, precision=0) -> int:
+        """Open one solve as a member; returns its slot.  Raises EvpError on a deck or start-up error."""
+        flags = (WRITE_FILES if write_files else 0) | (WRITE_CSV if csv_only else 0) | (MIXED if precision else 0)
+        slot = ctypes.c_int(-1)
+        _lib.check(_lib.load().evp_batch_add(self._h, str(fft_in).encode(), str(out_dir).encode(), int(mix), int(modal),
+                                             flags, ctypes.byref(slot)))
+        return int(slot.value)
+
+    def step(self, rounds: int = 1) -> int:
+        """Advance every running member by a few rounds of iterations; returns how many still run."""
+        n = ctypes.c_int(0)
+        _lib.check(_lib.load().evp_batch_step(self._h, int(rounds), ctypes.byref(n)))
+        return int(n.value)
+
+    def run(self) -> None:
+        while self.step(16) > 0:
+            pass
+
+    def status(self, slot: int) -> dict:
+        st, rep = ctypes.c_int(0), _lib.Report()
+        msg = ctypes.create_string_buffer(512)
+        _lib.check(_lib.load().evp_batch_status(self._h, int(slot), ctypes.byref(st), ctypes.byref(rep), msg, 512))
+        return {"state": "done" if st.value == 1 else "running", "status": rep.status, "macrosteps": rep.macrosteps,
+                "equilibrium_iters": rep.equilibrium_iters, "voxel_iters": rep.voxel_iters, "wall_s": rep.wall_s,
+                "grid": (rep.n1, rep.n2, rep.n3), "error": msg.value.decode(errors="replace")}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().evp_batch_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_files(ffts, out_dirs, mix=1, modal=0, csv_only=False, precision=0) -> list:
+    """Run every deck to its end as one batch (``evp_solve_files``); one Report per deck."""
+    n = len(ffts)
+    arr_in = (ctypes.c_char_p * n)(*[str(f).encode() for f in ffts])
+    arr_out = (ctypes.c_char_p * n)(*[str(o).encode() for o in out_dirs])
+    reps = (_lib.Report * n)()
+    flags = (WRITE_CSV if csv_only else WRITE_FILES) | (MIXED if precision else 0)
+    rc = _lib.load().evp_solve_files(n, arr_in, arr_out, int(mix), int(modal), flags, reps)
+    out = [reps[i] for i in range(n)]
+    if rc != 0 and all(r.status == 0 for r in out):
+        _lib.check(rc)
+    return out

@@ -119,6 +119,37 @@ int evp_green_apply(const double* d_tau, double* d_out, int n1, int n2, int n3, 
 int evp_green_apply_noalloc(const double* d_tau, double* d_out, int n1, int n2, int n3, const double* c0,
                             const double* s0, void* stream);
 
+/* ---- Batching: many solves advanced together (no counterpart in the reference, whose
+ * callers run one solver process per solve and two or three at once, utils/run.py:169-196,
+ * calibrate.py:1053-1057).
+ *
+ * Every equilibrium iteration of the batch is one launch per pass (stress average, the
+ * five FFT passes with the Green operator, correction, local Newton; per kernel variant
+ * and per 40 members) over all running members, whatever their grid sizes and material
+ * parameters, followed by a device-side controller that does each member's serial tail
+ * (averages, boundary-condition update, error norms, convergence and time-step rules)
+ * without the host; those launches are captured once in a CUDA graph and replayed.
+ * Members advance independently: one that converges writes its rows and starts its next
+ * increment while the others keep iterating; one that fails stops with its status and
+ * the others go on.  Each member's results are the same as when it runs alone. */
+typedef struct evp_batch evp_batch;
+int evp_batch_open(evp_batch** out);
+/* Add a solve (same deck, flags and files as evp_open; EVP_PROFILE is ignored).  *slot
+ * identifies it.  A deck or start-up error returns its status code (the slot, if
+ * any, is then finished with that status). */
+int evp_batch_add(evp_batch* b, const char* fft_in, const char* out_dir, int mix, int modal, int flags, int* slot);
+/* Advance the running members by `rounds` rounds of a few iterations each; *running gets the
+ * number of members still running. */
+int evp_batch_step(evp_batch* b, int rounds, int* running);
+/* *state: 0 running, 1 finished; rep->status is the member's status code once finished;
+ * msg (msgcap bytes, may be NULL) its error message. */
+int evp_batch_status(evp_batch* b, int slot, int* state, evp_report* rep, char* msg, int msgcap);
+int evp_batch_close(evp_batch* b);
+/* Run n decks as one batch to the end (the batched form of n evp_solve_file calls); reports[i]
+ * describes deck i; returns 0 or the first nonzero status.  flags 0: EVP_WRITE_FILES. */
+int evp_solve_files(int n, const char* const* fft_in, const char* const* out_dir, int mix, int modal, int flags,
+                    evp_report* reports);
+
 /* ---- Serving: a resident request loop (the reference has no counterpart; it
  * runs one solver process per request, utils/run.py:169-196, and calibrate.py
  * runs two or three such processes at once, calibrate.py:1053-1057).
