@@ -10,8 +10,9 @@ reference's (unshipped) microstructures.  A "step" is one macrostep
 updates.  Metric: voxel-iters/s = voxels x equilibrium iterations / device
 seconds (CUDA events on the solver's stream, max over ranks).  The state
 (~2 kB/voxel, 0.5 GB) is larger than the 126 MB L2, so no flush is needed.
-The line's "serving" object times a bounded sample of the served request stream
-(see serving_sample).
+The line's "batch" object times the calibration sweep batched against one solve
+after another (batch_sample), and its "serving" object the served request stream
+against the plain path (serving_stream).
 
 --gpus N > 1 runs N independent replicas (the solve does not shard), one
 process per GPU, and sums their voxel-iters.
@@ -247,43 +248,121 @@ def fft_vs_cufft(kd: dict, iters: int, n: int, dev) -> dict:
                     "cuFFT does the transforms only (torch.fft)"}
 
 
-def serving_sample(k: int, scale: float, rate: float) -> dict:
-    """The served request stream, bounded: the first k requests of the seeded stream (grid
-    edges 16-96, Arrhenius-scaled gamma0 at 475/525/575, creep 80-220 MPa) with their
-    increment counts scaled by `scale`, submitted to one resident server at their Poisson
-    arrival times (rate per s).  Latency = submit -> results.csv and diagnostics.csv written."""
+def _curves(path: Path):
+    import numpy as np
+
+    return np.loadtxt(path, delimiter=",", skiprows=1, ndmin=2)
+
+
+def _curve_err(a, b) -> float:
+    """Largest difference of the results.csv tensor curves (eav, sav, epav, eelav, vgrad, edotp), each
+    relative to its tensor's largest magnitude over the run."""
+    import numpy as np
+
+    if a.shape != b.shape:
+        return float("inf")
+    err = 0.0
+    for g in range(6):
+        cols = list(range(7 + 6 * g, 13 + 6 * g))
+        scale = float(np.max(np.abs(b[:, cols])))
+        if scale > 1e-30:
+            err = max(err, float(np.max(np.abs(a[:, cols] - b[:, cols])) / scale))
+    return err
+
+
+def batch_sample(k: int, nsteps: int) -> dict:
+    """The calibration sweep (configuration 4: grids 16^3-64^3, tau0, n and theta0 drawn per solve, creep
+    at 120 MPa) on its first k solves at the full increment count: all of them as one batch
+    (evp_solve_files) against one after the other through the plain path (evp_solve_file each, as the
+    reference's callers run one solver process per solve).  Same decks, same files; the batch members'
+    results.csv must equal the one-by-one ones."""
+    from creep_modeling_b200 import decks
+    from creep_modeling_b200 import solver as S
+
+    td = Path(tempfile.mkdtemp(prefix="evp_batch_"))
+    cases = [decks.case_c4(i, nsteps) for i in range(k)]
+    ffts = [decks.write_case(c, td / f"d{i}") for i, c in enumerate(cases)]
+    t0 = time.perf_counter()
+    reps = S.solve_files(ffts, [td / f"b{i}" for i in range(k)], mix=1, modal=0, csv_only=True)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    seq = [S.run_solver(f, td / f"s{i}", mix=1, modal=0) for i, f in enumerate(ffts)]
+    ts = time.perf_counter() - t0
+    same = all(_curve_err(_curves(td / f"b{i}" / "results.csv"), _curves(td / f"s{i}" / "results.csv")) == 0.0
+               for i in range(k))
+    vb = sum(r.voxel_iters for r in reps)
+    vs = sum(r.voxel_iters for r in seq)
+    return {"config": "calibration sweep (configuration 4)", "solves": k, "increments": nsteps,
+            "edges": [c.n for c in cases], "status": [r.status for r in reps],
+            "batched": {"wall_s": tb, "solves_per_hour": k / tb * 3600.0, "voxel_iters_per_s": vb / tb},
+            "one_by_one": {"wall_s": ts, "solves_per_hour": k / ts * 3600.0, "voxel_iters_per_s": vs / ts},
+            "speedup": ts / tb, "results_identical": bool(same),
+            "sample": f"first {k} of the 256 sweep solves, all {nsteps} increments, plain FP64"}
+
+
+def serving_stream(k: int, rate: float) -> dict:
+    """The served request stream (configuration 5: grid edges 16-96, Arrhenius-scaled gamma0 at
+    475/525/575, creep 80-220 MPa, 50-400 increments) on its first k requests at their full increment
+    counts, arriving as a Poisson stream of `rate` per s.  Served: one resident server, mixed precision,
+    every admitted solve in one batch (continuous batching); latency = arrival -> files written.
+    Plain: the FP64 path, one solve after the other in arrival order (evp_solve_file each, as the
+    reference's run.py runs one process per request), latency = arrival -> its solve's end.
+    Error: largest curve difference of every served (mixed) result against its plain FP64 result."""
     import numpy as np
 
     from creep_modeling_b200 import decks
+    from creep_modeling_b200 import solver as S
     from creep_modeling_b200.serve import Server
 
     td = Path(tempfile.mkdtemp(prefix="evp_serve_"))
-    cases = [decks.case_c5(i, scale) for i in range(k)]
+    cases = [decks.case_c5(i) for i in range(k)]
     ffts = [decks.write_case(c, td / f"r{i}") for i, c in enumerate(cases)]  # untimed
     arr = decks.stream_arrivals(k, rate)
-    with Server(0, 16) as srv:
+    # served
+    with Server(0, 64) as srv:
         t0 = time.perf_counter()
         tickets = []
         for i, f in enumerate(ffts):
             dt = arr[i] - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            tickets.append(srv.submit(f, td / f"o{i}", mix=1, modal=0, csv_only=True))
+            tickets.append(srv.submit(f, td / f"o{i}", mix=1, modal=0, precision=1, csv_only=True))
         sts = [srv.wait(t) for t in tickets]
         span = time.perf_counter() - t0
-    ok = [s for s in sts if s["status"] == 0]
-    lat = np.array([s["latency_s"] for s in ok])
-    return {
-        "requests": k, "completed": len(ok),
-        "failed": [{"request": i, "status": s["status"], "error": s["error"][:120]} for i, s in enumerate(sts) if s["status"] != 0],
-        "arrival_rate_per_s": rate, "increments_scale": scale,
-        "edges": [c.n for c in cases], "increments": [c.processes[0].nsteps for c in cases],
-        "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
-        "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
-        "solves_per_hour": len(ok) / span * 3600.0, "voxel_iters_per_s": sum(s["voxel_iters"] for s in ok) / span,
-        "span_s": span, "max_inflight": 16, "precision": "plain FP64 (error vs the FP64 path: 0 by construction)",
-        "sample": f"first {k} requests of the seeded stream, increments x{scale}, arrivals Poisson {rate}/s",
-    }
+    ok = [i for i, s in enumerate(sts) if s["status"] == 0]
+    lat = np.array([sts[i]["latency_s"] for i in ok])
+    served = {"completed": len(ok), "makespan_s": span, "solves_per_hour": len(ok) / span * 3600.0,
+              "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+              "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+              "voxel_iters_per_s": sum(sts[i]["voxel_iters"] for i in ok) / span,
+              "failed": [{"request": i, "status": s["status"], "error": s["error"][:120]} for i, s in enumerate(sts)
+                         if s["status"] != 0]}
+    # plain FP64, one by one in arrival order
+    t0 = time.perf_counter()
+    ends, vi, pok = [], 0, 0
+    for i, f in enumerate(ffts):
+        dt = arr[i] - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        try:
+            r = S.run_solver(f, td / f"p{i}", mix=1, modal=0)
+            vi += r.voxel_iters
+            pok += 1
+        except Exception:
+            pass
+        ends.append(time.perf_counter() - t0)
+    pspan = time.perf_counter() - t0
+    plat = np.array([ends[i] - arr[i] for i in range(k)])
+    plain = {"completed": pok, "makespan_s": pspan, "solves_per_hour": pok / pspan * 3600.0,
+             "p50_s": float(np.percentile(plat, 50)), "p99_s": float(np.percentile(plat, 99)),
+             "voxel_iters_per_s": vi / pspan}
+    errs = [_curve_err(_curves(td / f"o{i}" / "results.csv"), _curves(td / f"p{i}" / "results.csv")) for i in ok]
+    return {"config": "served request stream (configuration 5)", "requests": k, "arrival_rate_per_s": rate,
+            "edges": [c.n for c in cases], "increments": [c.processes[0].nsteps for c in cases],
+            "served_mixed_batched": served, "plain_fp64_one_by_one": plain,
+            "solves_per_hour_ratio": served["solves_per_hour"] / plain["solves_per_hour"],
+            "max_curve_rel_err_vs_fp64": max(errs) if errs else None,
+            "sample": f"first {k} requests of the seeded stream, full increment counts, Poisson arrivals {rate}/s"}
 
 
 def main(argv=None) -> int:
@@ -298,8 +377,9 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=25.0, help="seconds of timed CPU work in the cpu_baseline leg")
     ap.add_argument("--ref-budget", type=float, default=300.0, help="seconds of CPU time for --impl reference")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the served-stream sample (0: skip)")
-    ap.add_argument("--serve-scale", type=float, default=0.1, help="increment-count scale of the served-stream sample")
+    ap.add_argument("--serve-requests", type=int, default=12, help="requests of the served stream (0: skip)")
+    ap.add_argument("--batch-solves", type=int, default=8, help="solves of the calibration-sweep batch (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=150, help="increments of each sweep solve")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_env()
@@ -475,10 +555,16 @@ def main(argv=None) -> int:
     except Exception as exc:  # pragma: no cover
         fftcmp = {"error": str(exc)}
 
+    batch = None
+    if args.batch_solves > 0:
+        try:
+            batch = batch_sample(args.batch_solves, args.batch_steps)
+        except Exception as exc:  # pragma: no cover - reported, not hidden
+            batch = {"error": str(exc)}
     serving = None
     if args.serve_requests > 0:
         try:
-            serving = serving_sample(args.serve_requests, args.serve_scale, 20.0)
+            serving = serving_stream(args.serve_requests, 20.0)
         except Exception as exc:  # pragma: no cover - reported, not hidden
             serving = {"error": str(exc)}
 
@@ -490,7 +576,7 @@ def main(argv=None) -> int:
                    "increments_timed": f"{args.warmup + 1}-{args.warmup + args.steps}", "precision": "plain FP64",
                    "parallelism": f"replicas x{ws}", "l2": "state (~460 MB) larger than L2; no flush"},
         "wall_s": wall, "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-        "fft_vs_cufft": fftcmp, "serving": serving,
+        "fft_vs_cufft": fftcmp, "batch": batch, "serving": serving,
     }
     print(json.dumps(line), flush=True)
     if pg:

@@ -1,13 +1,18 @@
-// evp_server.cpp -- resident request loop over the solver's C ABI.
+// evp_server.cpp -- resident request loop over a batch of solves (continuous batching).
 //
 // The reference answers each request with a new solver process
 // (utils/run.py:169-196; calibrate.py runs two or three at once,
-// calibrate.py:1053-1057).  Here one process keeps a server: requests queue in
-// arrival order, a dispatcher thread admits them while the running solves'
-// device-memory estimates fit the budget, and every admitted solve runs on its
-// own host thread and CUDA stream (the solver creates a non-blocking stream and
-// allocates stream-ordered), so solves of different sizes overlap on the GPU.
+// calibrate.py:1053-1057).  Here one process keeps a server: requests are parsed on
+// the submitting thread and queue; one engine thread owns a Batch (evp_batch.h) on
+// the server's GPU.  Between rounds of batched iterations it admits queued requests
+// while their device-memory estimates fit the budget (the smallest remaining work
+// first: voxels times increments), so requests that arrive while others run join the
+// running batch as soon as memory and a slot free up, and their work shares the
+// launches of every solve already on the device.  Finished solves (their files
+// written) leave the batch at once.
 #include "../../include/evp.h"
+#include "evp_batch.h"
+#include "evp_deck.h"
 
 #include <cuda_runtime.h>
 
@@ -18,6 +23,7 @@
 #include <deque>
 #include <fstream>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -35,22 +41,13 @@ struct Request {
     double deadline_s = 0.0;  // wall-clock budget from admission (0: none)
     int n1 = 0, n2 = 0, n3 = 0;
     unsigned long long foot = 0;
+    double work = 0.0;  // voxels x increments of the deck: the admission order
+    std::shared_ptr<evp::Deck> deck;
     int state = 0, status = 0, macrosteps = 0;
     long long voxel_iters = 0;
     Clock::time_point t_submit, t_start, t_end;
     std::string error;
 };
-
-// Grid size from the deck's first two records (number of phases; nx ny nz).
-bool deck_grid(const std::string& fft, int& n1, int& n2, int& n3) {
-    std::ifstream f(fft);
-    if (!f) return false;
-    std::string line;
-    if (!std::getline(f, line)) return false;  // nph
-    if (!std::getline(f, line)) return false;
-    std::istringstream is(line);
-    return (bool)(is >> n1 >> n2 >> n3) && n1 > 0 && n2 > 0 && n3 > 0;
-}
 
 // Device memory of one solve, from the solver's allocations with the largest
 // slip-system count (24) and every optional field present: about 5.3 kB per
@@ -76,110 +73,133 @@ struct evp_server {
     std::condition_variable cv;  // any change of queue, admission or completion
     std::deque<unsigned long long> queue;
     std::map<unsigned long long, Request> reqs;
-    std::map<unsigned long long, std::thread> workers;
-    std::vector<unsigned long long> finished;  // workers to join
-    std::thread dispatcher;
-    unsigned long long budget = 0, used = 0, next_id = 1, arrivals = 0;
+    std::map<int, unsigned long long> slot_req;  // batch slot -> request
+    std::thread engine;
+    unsigned long long budget = 0, used = 0, next_id = 1;
     int max_inflight = 16, inflight = 0, device = 0;
     bool closing = false;
+    std::string fatal;  // a CUDA failure of the engine: every later request fails with it
 
-    void run_one(unsigned long long id) {
-        Request r;
-        {
-            std::lock_guard<std::mutex> lk(m);
-            r = reqs[id];
-        }
-        cudaSetDevice(device);
-        int rc = 0, macro = 0;
-        long long vi = 0;
-        std::string err;
-        evp_solve* h = nullptr;
-        rc = evp_open(r.fft.c_str(), r.out.c_str(), r.mix, r.modal, r.flags, &h);
-        if (rc != 0) {
-            err = evp_last_error();
-        } else {
-            if (r.deadline_s > 0.0) evp_set_deadline(h, r.deadline_s - secs(r.t_start, Clock::now()));
-            int done = 0;
-            while (true) {
-                rc = evp_advance(h, 1, &done);
-                if (rc != 0) {
-                    err = evp_last_error();
-                    break;
-                }
-                if (done == 0) break;
-            }
-            evp_report rep{};
-            evp_stats(h, &rep);
-            macro = rep.macrosteps;
-            vi = rep.voxel_iters;
-            evp_close(h);
-        }
-        std::lock_guard<std::mutex> lk(m);
-        Request& q = reqs[id];
+    void complete(Request& q, int status, const std::string& err, int macro, long long vi) {
         q.state = 2;
-        q.status = rc;
+        q.status = status;
         q.error = err;
         q.macrosteps = macro;
         q.voxel_iters = vi;
         q.t_end = Clock::now();
-        used -= q.foot;
-        inflight--;
-        finished.push_back(id);
-        cv.notify_all();
+        q.deck.reset();
     }
 
-    // join the threads of finished solves (called with the lock held; drops it while joining)
-    void reap(std::unique_lock<std::mutex>& lk) {
-        if (finished.empty()) return;
-        std::vector<std::thread> done;
-        for (auto id : finished) {
-            auto it = workers.find(id);
-            if (it != workers.end()) {
-                done.push_back(std::move(it->second));
-                workers.erase(it);
+    // called with the lock held; returns the queued request to admit next, or 0
+    unsigned long long pick() {
+        unsigned long long best = 0;
+        double best_work = 0.0;
+        for (auto id : queue) {
+            const Request& r = reqs[id];
+            if (used + r.foot > budget && inflight > 0) continue;  // a request larger than the budget runs alone
+            if (best == 0 || r.work < best_work) {
+                best = id;
+                best_work = r.work;
             }
         }
-        finished.clear();
-        lk.unlock();
-        for (auto& t : done) t.join();
-        lk.lock();
+        return best;
     }
 
-    void dispatch_loop() {
+    void engine_loop() {
+        cudaSetDevice(device);
+        std::unique_ptr<evp::Batch, void (*)(evp::Batch*)> batch(nullptr, evp::batch_destroy);
+        try {
+            batch.reset(evp::batch_create());
+        } catch (std::exception& e) {
+            std::lock_guard<std::mutex> lk(m);
+            fatal = e.what();
+        }
         std::unique_lock<std::mutex> lk(m);
         while (true) {
-            reap(lk);
-            cv.wait(lk, [&] { return closing || !queue.empty() || !finished.empty(); });
-            reap(lk);
-            if (queue.empty()) {
-                if (closing && inflight == 0) return;
-                if (closing) {
-                    cv.wait(lk, [&] { return inflight == 0 || !queue.empty() || !finished.empty(); });
-                    reap(lk);
-                    if (queue.empty() && inflight == 0) return;
-                }
-                continue;
-            }
-            // first request in arrival order that fits beside the running ones
-            bool admitted = false;
-            for (auto it = queue.begin(); it != queue.end() && inflight < max_inflight; ++it) {
-                Request& r = reqs[*it];
-                if (used + r.foot > budget && inflight > 0) continue;
-                // a request larger than the whole budget runs alone
+            // admission: smallest remaining work first, while slots and memory allow
+            while (batch && inflight < max_inflight && !queue.empty()) {
+                const unsigned long long id = pick();
+                if (id == 0) break;
+                for (auto it = queue.begin(); it != queue.end(); ++it)
+                    if (*it == id) {
+                        queue.erase(it);
+                        break;
+                    }
+                Request& r = reqs[id];
                 used += r.foot;
                 inflight++;
                 r.state = 1;
                 r.t_start = Clock::now();
-                const unsigned long long id = *it;
-                queue.erase(it);
-                workers.emplace(id, std::thread([this, id] { run_one(id); }));
-                admitted = true;
-                break;
+                std::shared_ptr<evp::Deck> dk = r.deck;
+                const std::string fft = r.fft, out = r.out;
+                const int mix = r.mix, modal = r.modal, flags = r.flags;
+                const double dl = r.deadline_s;
+                lk.unlock();
+                std::string err;
+                int slot = -1;
+                try {
+                    slot = evp::batch_add(batch.get(), std::move(*dk), fft, out, mix, modal, flags, dl, err);
+                } catch (std::exception& e) {
+                    err = e.what();
+                }
+                lk.lock();
+                Request& q = reqs[id];
+                int status = 0;
+                evp_report rep{};
+                const int st = slot >= 0 ? evp::batch_slot(batch.get(), slot, &status, &rep, &err) : 1;
+                if (slot < 0) status = -6;
+                if (st == 1) {  // failed at start-up (or a deck without steps)
+                    complete(q, status, err, rep.macrosteps, rep.voxel_iters);
+                    if (slot >= 0) evp::batch_remove(batch.get(), slot);
+                    used -= q.foot;
+                    inflight--;
+                    cv.notify_all();
+                } else {
+                    slot_req[slot] = id;
+                }
             }
-            if (!admitted) {  // until a solve ends or another request arrives
-                const unsigned long long a0 = arrivals;
-                cv.wait(lk, [&] { return !finished.empty() || arrivals != a0; });
+            if (!batch) {  // no device: fail what is queued
+                for (auto id : queue) complete(reqs[id], -6, fatal, 0, 0);
+                queue.clear();
+                cv.notify_all();
+                if (closing) return;
+                cv.wait(lk, [&] { return closing || !queue.empty(); });
+                continue;
             }
+            if (inflight == 0) {
+                if (closing && queue.empty()) break;
+                cv.wait(lk, [&] { return closing || !queue.empty(); });
+                continue;
+            }
+            lk.unlock();
+            std::string step_err;
+            try {
+                evp::batch_step(batch.get(), 1);
+            } catch (std::exception& e) {
+                step_err = e.what();
+            }
+            lk.lock();
+            for (auto it = slot_req.begin(); it != slot_req.end();) {
+                int status = 0;
+                evp_report rep{};
+                std::string err;
+                const int st = evp::batch_slot(batch.get(), it->first, &status, &rep, &err);
+                if (st == 1 || !step_err.empty()) {
+                    Request& q = reqs[it->second];
+                    if (st != 1) {
+                        status = -6;
+                        err = step_err;
+                    }
+                    complete(q, status, err, rep.macrosteps, rep.voxel_iters);
+                    evp::batch_remove(batch.get(), it->first);
+                    used -= q.foot;
+                    inflight--;
+                    it = slot_req.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+            cv.notify_all();
         }
     }
 };
@@ -213,7 +233,7 @@ int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const
     }
     s->budget = hbm_budget_bytes;
     s->max_inflight = max_inflight > 0 ? max_inflight : 16;
-    s->dispatcher = std::thread([s] { s->dispatch_loop(); });
+    s->engine = std::thread([s] { s->engine_loop(); });
     *out = s;
     return 0;
 }
@@ -236,16 +256,37 @@ int evp_submit_deadline(evp_server* srv, const char* fft_in, const char* out_dir
     r.precision = precision;
     r.flags = (flags & (EVP_WRITE_FILES | EVP_WRITE_CSV | EVP_VERBOSE)) | (precision == 1 ? EVP_MIXED : 0);
     r.deadline_s = deadline_s > 0.0 ? deadline_s : 0.0;
-    if (!deck_grid(r.fft, r.n1, r.n2, r.n3)) return srv_fail("evp_submit: cannot read the grid size from " + r.fft, -1);
-    r.foot = footprint(r.n1, r.n2, r.n3);
     r.t_submit = Clock::now();
+    // the deck is read here, on the submitting thread, so that admission only does device work
+    std::string perr;
+    int pcode = 0;
+    try {
+        r.deck = std::make_shared<evp::Deck>(evp::parse_deck(r.fft));
+        r.n1 = r.deck->n1;
+        r.n2 = r.deck->n2;
+        r.n3 = r.deck->n3;
+        long long steps = 0;
+        for (auto& p : r.deck->process) steps += p.nsteps;
+        r.work = (double)r.deck->nvox() * (double)(steps > 0 ? steps : 1);
+    } catch (evp::DeckError& e) {
+        perr = e.what();
+        pcode = e.code;
+    } catch (std::exception& e) {
+        perr = e.what();
+        pcode = -1;
+    }
+    r.foot = footprint(r.n1 > 0 ? r.n1 : 1, r.n2 > 0 ? r.n2 : 1, r.n3 > 0 ? r.n3 : 1);
     std::lock_guard<std::mutex> lk(srv->m);
     if (srv->closing) return srv_fail("evp_submit: server is closing", -7);
     r.id = srv->next_id++;
-    srv->reqs[r.id] = r;
-    srv->queue.push_back(r.id);
-    srv->arrivals++;
     *ticket = r.id;
+    if (pcode != 0) {  // a deck error: the request is done at once with the parser's status
+        srv->complete(r, pcode, perr, 0, 0);
+        srv->reqs[r.id] = r;
+    } else {
+        srv->reqs[r.id] = r;
+        srv->queue.push_back(r.id);
+    }
     srv->cv.notify_all();
     return 0;
 }
@@ -296,9 +337,7 @@ int evp_server_close(evp_server* srv) {
         srv->closing = true;
         srv->cv.notify_all();
     }
-    if (srv->dispatcher.joinable()) srv->dispatcher.join();
-    for (auto& kv : srv->workers)
-        if (kv.second.joinable()) kv.second.join();
+    if (srv->engine.joinable()) srv->engine.join();
     delete srv;
     return 0;
 }

@@ -155,13 +155,17 @@ int evp_solve_files(int n, const char* const* fft_in, const char* const* out_dir
  * runs two or three such processes at once, calibrate.py:1053-1057).
  *
  * A server keeps every admitted solve's fields on the device until the solve
- * ends and writes the same files as evp_solve_file.  Requests wait in arrival
- * order; a request is admitted as soon as fewer than max_inflight solves run
- * and its estimated device footprint fits the budget beside the running ones
- * (a later, smaller request may go first when the oldest one does not fit).
- * Admitted solves run concurrently, each on its own CUDA stream and host
- * thread, so the kernels of solves of different grid sizes overlap on the GPU
- * and one solve's host work hides behind another's device work.  A solve's
+ * ends and writes the same files as evp_solve_file.  evp_submit reads the deck
+ * on the caller's thread (a deck error makes the request done at once with its
+ * status); requests then queue.  One engine thread runs all admitted solves as
+ * one batch (the evp_batch_* form: every equilibrium iteration is one launch per
+ * pass over all of them, whatever their grid sizes).  Between rounds of a few
+ * iterations it admits queued requests, the one with the least work (voxels x
+ * increments) first, while fewer than max_inflight solves run and the request's
+ * estimated device footprint fits the budget beside the running ones; a request
+ * larger than the whole budget runs alone.  So requests that arrive while others
+ * are on the GPU join the running batch as soon as a slot and memory free up
+ * (continuous batching), and a solve that finishes leaves it at once.  A solve's
  * results do not depend on what else runs beside it. */
 typedef struct evp_server evp_server;
 
