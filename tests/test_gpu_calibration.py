@@ -51,3 +51,34 @@ def test_batch_scores_every_candidate_and_load(tmp_path):
     assert base[0] < base[2]
     for r in res:
         assert r["loss"] == pytest.approx(r["base"] + 1e-3 * r["avg_iters"], rel=1e-12)
+
+
+def test_batch_scores_match_the_oracle(tmp_path, oracle_lib):
+    """Every candidate x load solve of the served batch against the CPU FP64 oracle on the same
+    deck: the results.csv rows within the parity bar (identical iteration counts, 1e-8 per
+    column) and the creep objective of each solve within 1e-8 of the oracle's."""
+    import numpy as np
+
+    from creep_modeling_b200.solver import load_results
+    from tests import parity
+
+    with Server(0, 8) as srv:
+        ref_jobs = _jobs(tmp_path / "a")
+        assert [r["status"] for r in cal.evaluate_batch(srv, ref_jobs)] == [0] * 6
+        ref = cal.read_results(tmp_path / "a" / "cand0" / "creep150" / "out")
+        tgt = cal.CreepTarget(150, ref["sim_time"], ref["epav33"])
+        jobs = _jobs(tmp_path / "b", tgt)
+        res = cal.evaluate_batch(srv, jobs)
+    for job, r in zip(jobs, res):
+        odir = job.out_dir.parent / "oracle"
+        o = oracle_lib.OracleSolve(job.fft_in, out_dir=str(odir), mix=1, modal=0, write_files=True)
+        o.run()
+        o.close()
+        rg, ro = load_results(job.out_dir / "results.csv"), load_results(odir / "results.csv")
+        dg = np.loadtxt(job.out_dir / "diagnostics.csv", delimiter=",", skiprows=1, ndmin=2)
+        do = np.loadtxt(odir / "diagnostics.csv", delimiter=",", skiprows=1, ndmin=2)
+        parity.assert_rows_match(rg, ro, dg, do)
+        base_o = cal.creep_objective(cal.read_results(odir), tgt)
+        # the objective is a mean absolute difference of plastic-strain curves: compare it on the curves' scale
+        scale = float(np.max(np.abs(ref["epav33"])))
+        assert abs(r["base"] - base_o) <= 1e-8 * scale, (r["base"], base_o)
