@@ -14,7 +14,7 @@ EXPORTED = (
     "evp_kernel_times", "evp_green_apply", "evp_green_apply_noalloc", "evp_last_error", "evp_version",
     "evp_server_open", "evp_submit", "evp_submit_deadline", "evp_poll", "evp_wait", "evp_server_close",
     "evp_set_deadline", "evp_kernel_launches", "evp_newton_stats",
-    "evp_batch_open", "evp_batch_add", "evp_batch_step", "evp_batch_status", "evp_batch_close", "evp_solve_files",
+    "evp_tune_cache", "evp_batch_open", "evp_batch_add", "evp_batch_step", "evp_batch_status", "evp_batch_close", "evp_solve_files",
 )
 
 STATUS = {
@@ -100,6 +100,8 @@ def load(path: Path | str | None = None):
     L.evp_kernel_times.restype = ctypes.c_int
     L.evp_newton_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.evp_newton_stats.restype = ctypes.c_int
+    L.evp_tune_cache.argtypes = [ctypes.c_char_p]
+    L.evp_tune_cache.restype = ctypes.c_int
     ip = ctypes.POINTER(ctypes.c_int)
     L.evp_batch_open.argtypes = [ctypes.POINTER(vp)]
     L.evp_batch_open.restype = ctypes.c_int

@@ -20,8 +20,13 @@
 #include "evp_math.cuh"
 
 #include <algorithm>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace evp {
 
@@ -838,6 +843,50 @@ void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
     else green_apply_rs<1>(d, pl1, pl2, pl3, tau, out, c0, s0, st);
 }
 
+// ---------------------------------------------------------------- measured tile choice (autotuner)
+// For the spectral passes whose work per pencil does not depend on the tile (x forward,
+// y, z with the Green operator: no reduction inside), the tile can be picked by timing the
+// candidates on the device.  fft_autotune does that for a solve's grid at open time when a
+// tile cache file is set (the executable's --fftw_save path, the server's tune_cache) and
+// the grid is not in it yet; the choice is kept for the process and appended to the file,
+// so later solves of the same grid, here or in another process, read it instead of timing
+// again.  Without a cache file the passes use the occupancy / wave-count model.  The tile
+// does not change any result: every pencil is transformed by the same arithmetic.
+struct TuneKey {
+    int pass, rs, ct, n1, n2, n3;
+    bool operator<(const TuneKey& o) const {
+        const int a[6] = {pass, rs, ct, n1, n2, n3}, b[6] = {o.pass, o.rs, o.ct, o.n1, o.n2, o.n3};
+        for (int i = 0; i < 6; i++)
+            if (a[i] != b[i]) return a[i] < b[i];
+        return false;
+    }
+};
+enum : int { TUNE_XFWD = 0, TUNE_Y = 1, TUNE_ZGREEN = 2 };
+static std::mutex g_tune_m;
+static std::map<TuneKey, int> g_tuned;
+static std::string g_tune_path;
+
+static int tuned_tile(int pass, int rs, int ct, const Dev& d) {
+    std::lock_guard<std::mutex> lk(g_tune_m);
+    auto it = g_tuned.find(TuneKey{pass, rs, ct, d.n1, d.n2, d.n3});
+    return it == g_tuned.end() ? -1 : it->second;
+}
+
+void fft_tune_cache(const std::string& path) {
+    std::lock_guard<std::mutex> lk(g_tune_m);
+    g_tune_path = path;
+    if (path.empty()) return;
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line)) {  // "evp-tile pass rs ct n1 n2 n3 tile"
+        std::istringstream is(line);
+        std::string tag;
+        TuneKey k{};
+        int t = 0;
+        if ((is >> tag >> k.pass >> k.rs >> k.ct >> k.n1 >> k.n2 >> k.n3 >> t) && tag == "evp-tile" && t > 0) g_tuned[k] = t;
+    }
+}
+
 // Launch shape of one pass over one solve: grid (gx, gy, gz), tile (rows or pencils per
 // block), threads per block and dynamic shared memory.  The single-solve launchers and the
 // batched launches use the same shapes, so a solve's blocks do the same work either way.
@@ -850,9 +899,11 @@ static FftShape x_fwd_shape(const Dev& d, const FftPlan1D& pl) {
     static const int mx = kernel_max_threads((const void*)k_fft_x_fwd<RS, CT>);
     int thr = 0;
     const long long npr = ((long long)d.n2 * d.n3 + 1) / 2;
-    const int G = choose_tile((const void*)k_fft_x_fwd<RS, CT>, x_rows_per_block(d.n1), 9, pl, RS, 128, mx,
-                              [&](int g) { return (npr + g - 1) / g; },
-                              [&](int g) { return (size_t)9 * g * d.n1 * sizeof(CT); }, thr);
+    const int tt = tuned_tile(TUNE_XFWD, RS, sizeof(CT) == sizeof(float2), d);
+    const int G = tt > 0 ? fit_tile(tt, 9, pl, RS, 128, mx, thr)
+                         : choose_tile((const void*)k_fft_x_fwd<RS, CT>, x_rows_per_block(d.n1), 9, pl, RS, 128, mx,
+                                       [&](int g) { return (npr + g - 1) / g; },
+                                       [&](int g) { return (size_t)9 * g * d.n1 * sizeof(CT); }, thr);
     const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
     return FftShape{(npairs + G - 1) / G, 1, 1, G, thr, (size_t)9 * G * d.n1 * sizeof(CT)};
 }
@@ -877,9 +928,11 @@ template <int RS, class CT>
 static FftShape y_shape(const Dev& d, const FftPlan1D& pl, int ncomp) {
     static const int mx = std::min(kernel_max_threads((const void*)k_fft_y<true, RS, CT>), kernel_max_threads((const void*)k_fft_y<false, RS, CT>));
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_y<false, RS, CT>, y_tile(d), 1, pl, RS, 64, mx,
-                              [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n3 * ncomp; },
-                              [&](int t) { return (size_t)t * d.n2 * sizeof(CT); }, thr);
+    const int tt = ncomp == 9 ? tuned_tile(TUNE_Y, RS, sizeof(CT) == sizeof(float2), d) : -1;
+    const int T = tt > 0 ? fit_tile(tt, 1, pl, RS, 64, mx, thr)
+                         : choose_tile((const void*)k_fft_y<false, RS, CT>, y_tile(d), 1, pl, RS, 64, mx,
+                                       [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n3 * ncomp; },
+                                       [&](int t) { return (size_t)t * d.n2 * sizeof(CT); }, thr);
     return FftShape{(d.n1h + T - 1) / T, d.n3, ncomp, T, thr, (size_t)T * d.n2 * sizeof(CT)};
 }
 template <int RS, class CT>
@@ -904,9 +957,11 @@ template <int RS, class CT>
 static FftShape z_green_shape(const Dev& d, const FftPlan1D& pl) {
     static const int mx = kernel_max_threads((const void*)k_fft_z_green<RS, CT>);
     int thr = 0;
-    const int T = choose_tile((const void*)k_fft_z_green<RS, CT>, z_tile(d), 9, pl, RS, 128, mx,
-                              [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
-                              [&](int t) { return (size_t)9 * t * d.n3 * sizeof(CT); }, thr);
+    const int tt = tuned_tile(TUNE_ZGREEN, RS, sizeof(CT) == sizeof(float2), d);
+    const int T = tt > 0 ? fit_tile(tt, 9, pl, RS, 128, mx, thr)
+                         : choose_tile((const void*)k_fft_z_green<RS, CT>, z_tile(d), 9, pl, RS, 128, mx,
+                                       [&](int t) { return (long long)((d.n1h + t - 1) / t) * d.n2; },
+                                       [&](int t) { return (size_t)9 * t * d.n3 * sizeof(CT); }, thr);
     return FftShape{(d.n1h + T - 1) / T, d.n2, 1, T, thr, (size_t)9 * T * d.n3 * sizeof(CT)};
 }
 template <int RS, class CT>
@@ -987,6 +1042,110 @@ void launch_fft_x_inv(const Dev& d, const FftPlan1D& pl, int mode, const XinvPar
     const bool f32 = prec != 0 && mode == 0;  // the grid-update chain (mode 1) stays FP64
     if (plan_pow2(pl)) f32 ? x_inv_rs<0, float2>(d, pl, mode, p, st) : x_inv_rs<0, double2>(d, pl, mode, p, st);
     else f32 ? x_inv_rs<1, float2>(d, pl, mode, p, st) : x_inv_rs<1, double2>(d, pl, mode, p, st);
+}
+
+// Time every candidate tile of the three tunable passes on this solve's grid (the solve's own
+// state: the spectrum is scratch between iterations, and c0 / s0 are set) and keep the fastest.
+// Candidates: every tile up to the model's upper bound that fits one block (fit_tile); each
+// is launched once untimed and three times between CUDA events on the solve's stream.
+template <class F>
+static float time_launches(F&& launch, cudaStream_t st) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    launch();
+    cudaEventRecord(a, st);
+    for (int i = 0; i < 3; i++) launch();
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+static std::vector<int> tile_candidates(int T0) {
+    std::vector<int> c;
+    for (int t = 1; t <= T0; t++)
+        if (t <= 8 || t == T0 || t % 4 == 0) c.push_back(t);
+    return c;
+}
+template <int RS, class CT>
+static void autotune_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* c0,
+                        const double* s0, cudaStream_t st, std::vector<std::pair<TuneKey, int>>& found) {
+    const int ct = sizeof(CT) == sizeof(float2) ? 1 : 0;
+    const int nrows = d.n2 * d.n3, npairs = (nrows + 1) / 2;
+    auto pick = [&](int pass, int T0, auto&& fits, auto&& launch) {
+        if (tuned_tile(pass, RS, ct, d) > 0) return;
+        int best = -1;
+        float best_ms = 0.f;
+        for (int t : tile_candidates(T0)) {
+            int thr = 0;
+            if (!fits(t, thr)) continue;
+            const float ms = time_launches([&] { launch(t, thr); }, st);
+            if (cudaGetLastError() != cudaSuccess) continue;
+            if (best < 0 || ms < best_ms) {
+                best = t;
+                best_ms = ms;
+            }
+        }
+        if (best > 0) found.push_back({TuneKey{pass, RS, ct, d.n1, d.n2, d.n3}, best});
+    };
+    const int mx_x = kernel_max_threads((const void*)k_fft_x_fwd<RS, CT>);
+    pick(TUNE_XFWD, x_rows_per_block(d.n1),
+         [&](int t, int& thr) {
+             try { return fit_tile(t, 9, pl1, RS, 128, mx_x, thr) == t; } catch (std::exception&) { return false; }
+         },
+         [&](int t, int thr) {
+             k_fft_x_fwd<RS, CT><<<(npairs + t - 1) / t, thr, (size_t)9 * t * d.n1 * sizeof(CT), st>>>(d, pl1, t, 0, OFF_SGAVG);
+         });
+    const int mx_y = std::min(kernel_max_threads((const void*)k_fft_y<true, RS, CT>), kernel_max_threads((const void*)k_fft_y<false, RS, CT>));
+    pick(TUNE_Y, y_tile(d),
+         [&](int t, int& thr) {
+             try { return fit_tile(t, 1, pl2, RS, 64, mx_y, thr) == t; } catch (std::exception&) { return false; }
+         },
+         [&](int t, int thr) {
+             k_fft_y<false, RS, CT><<<dim3((d.n1h + t - 1) / t, d.n3, 9), thr, (size_t)t * d.n2 * sizeof(CT), st>>>(d, pl2, t);
+         });
+    const int mx_z = kernel_max_threads((const void*)k_fft_z_green<RS, CT>);
+    pick(TUNE_ZGREEN, z_tile(d),
+         [&](int t, int& thr) {
+             try { return fit_tile(t, 9, pl3, RS, 128, mx_z, thr) == t; } catch (std::exception&) { return false; }
+         },
+         [&](int t, int thr) {
+             k_fft_z_green<RS, CT><<<dim3((d.n1h + t - 1) / t, d.n2), thr, (size_t)9 * t * d.n3 * sizeof(CT), st>>>(d, pl3, t, c0, s0);
+         });
+}
+
+int fft_autotune(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* c0,
+                 const double* s0, int prec, cudaStream_t st) {
+    {
+        std::lock_guard<std::mutex> lk(g_tune_m);
+        if (g_tune_path.empty()) return 0;
+    }
+    std::vector<std::pair<TuneKey, int>> found;
+    // each pass takes the radix set of its own axis (x forward: axis 1, y: axis 2, z: axis 3); tuning
+    // both sets is cheap and covers whichever each axis needs
+    for (int w = 0; w < (prec ? 2 : 1); w++) {
+        if (w == 0) {
+            autotune_rs<0, double2>(d, pl1, pl2, pl3, c0, s0, st, found);
+            autotune_rs<1, double2>(d, pl1, pl2, pl3, c0, s0, st, found);
+        } else {
+            autotune_rs<0, float2>(d, pl1, pl2, pl3, c0, s0, st, found);
+            autotune_rs<1, float2>(d, pl1, pl2, pl3, c0, s0, st, found);
+        }
+    }
+    if (found.empty()) return 0;
+    std::lock_guard<std::mutex> lk(g_tune_m);
+    std::ofstream f(g_tune_path, std::ios::app);
+    for (auto& kv : found) {
+        if (g_tuned.count(kv.first)) continue;
+        g_tuned[kv.first] = kv.second;
+        const TuneKey& k = kv.first;
+        f << "evp-tile " << k.pass << ' ' << k.rs << ' ' << k.ct << ' ' << k.n1 << ' ' << k.n2 << ' ' << k.n3 << ' '
+          << kv.second << '\n';
+    }
+    return (int)found.size();
 }
 
 // ---------------------------------------------------------------- batched launches of the iteration's spectral passes

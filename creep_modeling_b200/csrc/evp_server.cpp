@@ -216,8 +216,8 @@ static int srv_fail(const std::string& m, int code) {
 extern "C" {
 
 int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const char* tune_cache, evp_server** out) {
-    (void)tune_cache;
     if (!out) return srv_fail("evp_server_open: null argument", -7);
+    if (tune_cache && tune_cache[0] && evp_tune_cache(tune_cache) != 0) return -7;
     *out = nullptr;
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return srv_fail("no CUDA device available", -6);

@@ -42,7 +42,7 @@ void set_last_error(const std::string& m) { g_last_error = m; }
         if (e_ != cudaSuccess) throw SolveError(std::string("CUDA error: ") + cudaGetErrorString(e_), -6); \
     } while (0)
 
-static void mkdir_p(const std::string& dir) {
+void mkdir_p(const std::string& dir) {
     std::string cur;
     for (size_t i = 0; i <= dir.size(); i++) {
         if (i == dir.size() || dir[i] == '/')
@@ -304,6 +304,7 @@ public:
         b66_to_t4(s066, s0);
         std::memcpy(de_ds, s0, sizeof(de_ds));
         upload_c0();
+        fft_autotune(d, pl1, pl2, pl3, d_c0, d_s0, prec, st);  // no-op without a tile cache file
         if (write_files) write_headers();
         for (auto& p : dk.process) total_macrosteps += p.nsteps;
         imacroloop = 1;
@@ -1690,9 +1691,23 @@ int evp_solve_files(int n, const char* const* fft_in, const char* const* out_dir
     return worst;
 }
 
+int evp_tune_cache(const char* path) {
+    try {
+        const std::string p = path ? path : "";
+        if (!p.empty()) {
+            const std::string dir = std::filesystem::path(p).parent_path().string();
+            if (!dir.empty()) evp::mkdir_p(dir);
+        }
+        evp::fft_tune_cache(p);
+    } catch (std::exception& e) {
+        return fail(e.what(), -7);
+    }
+    return 0;
+}
+
 int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const char* fftw_save, int mix, int modal, evp_report* report) {
     (void)nthreads;
-    (void)fftw_save;
+    if (fftw_save && fftw_save[0]) evp_tune_cache(fftw_save);
     auto t0 = std::chrono::steady_clock::now();
     evp_solve* h = nullptr;
     int rc = evp_open(fft_in, out_dir, mix, modal, EVP_WRITE_FILES, &h);

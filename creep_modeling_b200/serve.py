@@ -42,12 +42,14 @@ class Server:
     """A resident request loop on the current GPU.
 
     hbm_budget_bytes: device memory the running solves may hold together (0: 85 %
-    of the free memory); max_inflight: solves running at once."""
+    of the free memory); max_inflight: solves running at once; tune_cache: the FFT
+    passes' tile cache file (see solver.tune_cache)."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 16):
+    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 16, tune_cache=None):
         L = _lib.load()
         h = ctypes.c_void_p()
-        _lib.check(L.evp_server_open(int(hbm_budget_bytes), int(max_inflight), None, ctypes.byref(h)))
+        tc = str(tune_cache).encode() if tune_cache else None
+        _lib.check(L.evp_server_open(int(hbm_budget_bytes), int(max_inflight), tc, ctypes.byref(h)))
         self._h = h
         self._lock = threading.Lock()
 

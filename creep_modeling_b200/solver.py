@@ -46,6 +46,12 @@ def run_solver(fft_in, out_dir="evpfft_outputs/", nthreads=0, fftw_save="", mix=
     return rep
 
 
+def tune_cache(path) -> None:
+    """Tile cache of the FFT passes for every later solve in this process (``evp_tune_cache``):
+    grids not in the file are timed on the device at open and appended; None or "": no cache."""
+    _lib.check(_lib.load().evp_tune_cache(str(path).encode() if path else b""))
+
+
 class Solve:
     """A device-resident solve advanced macrostep by macrostep."""
 

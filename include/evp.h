@@ -48,10 +48,18 @@ typedef struct evp_report {
 
 /* Whole solve with the executable's semantics: replaces one
  * `LS-EVPFFT --in fft_in --out out_dir --mix mix --modal modal` process
- * (LS-EVPFFT.f90:87-595).  nthreads and fftw_save are accepted for the same
- * command line and ignored (there is no FFTW planner). */
+ * (LS-EVPFFT.f90:87-595).  nthreads is accepted for the same command line and
+ * ignored.  fftw_save, the reference's FFTW wisdom file (fourier_functions.f90:35-66),
+ * names the tile cache of the FFT passes here (evp_tune_cache); NULL or "": none. */
 int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const char* fftw_save, int mix, int modal,
                    evp_report* report);
+
+/* Tile cache of the spectral passes for every later open in this process (the
+ * counterpart of FFTW's wisdom file; path NULL or "": none).  With a cache, opening a
+ * solve whose grid is not in the file yet times the candidate tiles of the x-forward,
+ * y and z-with-Green-operator passes on the device and appends the fastest; later
+ * solves of that grid read it.  The tile changes no result.  Its directory is created. */
+int evp_tune_cache(const char* path);
 
 /* Step-wise form of the same solve, for tests and the serving loop.
  * evp_open = load_input + initial_guess + start-up c0 (LS-EVPFFT.f90:144-178);
@@ -184,7 +192,7 @@ typedef struct evp_status {
 
 /* hbm_budget_bytes: device memory the running solves may hold together (0: 85 % of
  * the free memory at open).  max_inflight: solves run at once (<= 0: 16).
- * tune_cache: reserved for a tile-shape cache; may be NULL. */
+ * tune_cache: the tile cache of the FFT passes (as evp_tune_cache); may be NULL. */
 int evp_server_open(unsigned long long hbm_budget_bytes, int max_inflight, const char* tune_cache, evp_server** out);
 /* Queue one solve (same deck and flags as evp_solve_file; precision 0 = plain FP64,
  * 1 = mixed precision as EVP_MIXED).
