@@ -177,16 +177,38 @@ __device__ void control_one(IterCtl& c, const double* red, int err) {
     }
 }
 
-__global__ void k_control(const BatchSolve* __restrict__ E, int n, int* __restrict__ events) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per solve: the warp copies the solve's control block and the sums it reads into
+// shared memory (coalesced), lane 0 does the serial tail there, and the warp writes the block
+// back; the serial code then waits on shared memory instead of one global load after another.
+constexpr int kCtlWords = (int)(sizeof(IterCtl) / 8);
+static_assert(sizeof(IterCtl) % 8 == 0, "IterCtl is copied in 8-byte words");
+
+__global__ void __launch_bounds__(32) k_control(const BatchSolve* __restrict__ E, int n, int* __restrict__ events) {
+    const int i = blockIdx.x;
     if (i >= n) return;
-    IterCtl& c = *E[i].ctl;
-    if (c.active) control_one(c, E[i].d.red, *(volatile int*)E[i].d.err);
-    events[i] = c.active ? EV_RUNNING : c.event;
+    __shared__ IterCtl c;
+    __shared__ double red[OFF_NEWTON + 14];
+    __shared__ int err;
+    IterCtl* g = E[i].ctl;
+    unsigned long long* cw = reinterpret_cast<unsigned long long*>(&c);
+    const unsigned long long* gw = reinterpret_cast<const unsigned long long*>(g);
+    for (int w = threadIdx.x; w < kCtlWords; w += 32) cw[w] = gw[w];
+    const double* r = E[i].d.red;
+    for (int k = OFF_CORR + threadIdx.x; k < OFF_NEWTON + 14; k += 32) red[k] = r[k];
+    if (threadIdx.x == 0) err = *(volatile int*)E[i].d.err;
+    __syncwarp();
+    const bool run = c.active != 0;
+    if (run && threadIdx.x == 0) control_one(c, red, err);
+    __syncwarp();
+    if (run) {
+        unsigned long long* gwo = reinterpret_cast<unsigned long long*>(g);
+        for (int w = threadIdx.x; w < kCtlWords; w += 32) gwo[w] = cw[w];
+    }
+    if (threadIdx.x == 0) events[i] = c.active ? EV_RUNNING : c.event;
 }
 
 void launch_control(const BatchSolve* E, int n, int* events, cudaStream_t st) {
-    k_control<<<(n + 63) / 64, 64, 0, st>>>(E, n, events);
+    k_control<<<n, 32, 0, st>>>(E, n, events);
 }
 
 }  // namespace evp

@@ -261,9 +261,9 @@ void launch_batched_fft(const BatchLaunch& L, const BatchParams& P, cudaStream_t
 // the serial tail of one iteration for n solves (evp_control.cu); events[i] = EV_* or a status code
 void launch_control(const BatchSolve* E, int n, int* events, cudaStream_t st);
 
-// Measured tile choice of the spectral passes (evp_fft.cu): the cache file (empty: none, the
-// occupancy model decides), and the timing of the candidates for a solve's grid at open
-// (returns how many pass shapes were tuned; 0 without a cache file or when all were cached).
+// Measured tile choice of the spectral passes (evp_fft.cu): the cache file (empty: none) and
+// the timing of the candidates for a solve's grid at open (returns how many pass shapes were
+// tuned; 0 when the process or the file knew them all).
 void fft_tune_cache(const std::string& path);
 int fft_autotune(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* c0,
                  const double* s0, int prec, cudaStream_t st);

@@ -20,6 +20,7 @@
 #include "evp_math.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <fstream>
 #include <map>
 #include <mutex>
@@ -845,13 +846,13 @@ void launch_green_apply(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
 
 // ---------------------------------------------------------------- measured tile choice (autotuner)
 // For the spectral passes whose work per pencil does not depend on the tile (x forward,
-// y, z with the Green operator: no reduction inside), the tile can be picked by timing the
-// candidates on the device.  fft_autotune does that for a solve's grid at open time when a
-// tile cache file is set (the executable's --fftw_save path, the server's tune_cache) and
-// the grid is not in it yet; the choice is kept for the process and appended to the file,
-// so later solves of the same grid, here or in another process, read it instead of timing
-// again.  Without a cache file the passes use the occupancy / wave-count model.  The tile
-// does not change any result: every pencil is transformed by the same arithmetic.
+// y, z with the Green operator: no reduction inside), the tile is picked by timing the
+// candidates on the device.  fft_autotune does that for a solve's grid at open time, once
+// per grid and process (a few milliseconds); with a tile cache file (the executable's
+// --fftw_save path, the server's tune_cache) the choices are also appended to the file and
+// read back by later processes instead of timing again.  The occupancy / wave-count model
+// gives the candidates' upper bound and the tile of the passes that are not tuned.  The
+// tile does not change any result: every pencil is transformed by the same arithmetic.
 struct TuneKey {
     int pass, rs, ct, n1, n2, n3;
     bool operator<(const TuneKey& o) const {
@@ -1119,10 +1120,8 @@ static void autotune_rs(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2
 
 int fft_autotune(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const FftPlan1D& pl3, const double* c0,
                  const double* s0, int prec, cudaStream_t st) {
-    {
-        std::lock_guard<std::mutex> lk(g_tune_m);
-        if (g_tune_path.empty()) return 0;
-    }
+    const char* off = getenv("EVP_TUNE");  // EVP_TUNE=0: keep the model's tiles (for comparisons)
+    if (off && off[0] == '0') return 0;
     std::vector<std::pair<TuneKey, int>> found;
     // each pass takes the radix set of its own axis (x forward: axis 1, y: axis 2, z: axis 3); tuning
     // both sets is cheap and covers whichever each axis needs
@@ -1137,13 +1136,15 @@ int fft_autotune(const Dev& d, const FftPlan1D& pl1, const FftPlan1D& pl2, const
     }
     if (found.empty()) return 0;
     std::lock_guard<std::mutex> lk(g_tune_m);
-    std::ofstream f(g_tune_path, std::ios::app);
+    std::ofstream f;
+    if (!g_tune_path.empty()) f.open(g_tune_path, std::ios::app);
     for (auto& kv : found) {
         if (g_tuned.count(kv.first)) continue;
         g_tuned[kv.first] = kv.second;
         const TuneKey& k = kv.first;
-        f << "evp-tile " << k.pass << ' ' << k.rs << ' ' << k.ct << ' ' << k.n1 << ' ' << k.n2 << ' ' << k.n3 << ' '
-          << kv.second << '\n';
+        if (f.is_open())
+            f << "evp-tile " << k.pass << ' ' << k.rs << ' ' << k.ct << ' ' << k.n1 << ' ' << k.n2 << ' ' << k.n3 << ' '
+              << kv.second << '\n';
     }
     return (int)found.size();
 }

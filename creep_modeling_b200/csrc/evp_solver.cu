@@ -304,7 +304,7 @@ public:
         b66_to_t4(s066, s0);
         std::memcpy(de_ds, s0, sizeof(de_ds));
         upload_c0();
-        fft_autotune(d, pl1, pl2, pl3, d_c0, d_s0, prec, st);  // no-op without a tile cache file
+        fft_autotune(d, pl1, pl2, pl3, d_c0, d_s0, prec, st);  // once per grid and process
         if (write_files) write_headers();
         for (auto& p : dk.process) total_macrosteps += p.nsteps;
         imacroloop = 1;

@@ -55,10 +55,11 @@ int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const 
                    evp_report* report);
 
 /* Tile cache of the spectral passes for every later open in this process (the
- * counterpart of FFTW's wisdom file; path NULL or "": none).  With a cache, opening a
- * solve whose grid is not in the file yet times the candidate tiles of the x-forward,
- * y and z-with-Green-operator passes on the device and appends the fastest; later
- * solves of that grid read it.  The tile changes no result.  Its directory is created. */
+ * counterpart of FFTW's wisdom file; path NULL or "": none).  Opening a solve whose
+ * grid this process has not seen times the candidate tiles of the x-forward, y and
+ * z-with-Green-operator passes on the device (a few milliseconds) unless the cache
+ * file has them; the fastest are kept for the process and appended to the file, so
+ * later processes read them.  The tile changes no result.  Its directory is created. */
 int evp_tune_cache(const char* path);
 
 /* Step-wise form of the same solve, for tests and the serving loop.

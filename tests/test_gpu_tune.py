@@ -1,9 +1,10 @@
 """The FFT tile autotuner and its cache file (the counterpart of the reference's FFTW wisdom).
 
-A solve opened while a tile cache is set times the candidate tiles of the x-forward, y
-and z-with-Green-operator passes for its grid and appends the fastest to the file; a
-second solve of the same grid reads them instead of timing again.  The tile changes
-no result, so the tuned solves' rows equal the untuned ones exactly.
+Opening a solve whose grid the process has not seen times the candidate tiles of the
+x-forward, y and z-with-Green-operator passes and keeps the fastest; with a cache file
+set they are appended to it, and a later solve of the same grid reads them instead of
+timing again.  The tile changes no result: rows with tuned tiles equal the rows with
+the occupancy model's tiles (EVP_TUNE=0) exactly.
 """
 import numpy as np
 import pytest
@@ -24,11 +25,13 @@ def _rows(fft, n):
     return np.array(rows)
 
 
-def test_tuned_tiles_are_cached_and_change_nothing(tmp_path):
+def test_tuned_tiles_are_cached_and_change_nothing(tmp_path, monkeypatch):
     case = decks.case_c1(nsteps=3)
-    case.n, case.ngrains = (24, 20, 12), 20
+    case.n, case.ngrains = (20, 18, 10), 16  # a grid no other test uses, so this process has not tuned it
     fft = decks.write_case(case, tmp_path / "deck")
-    before = _rows(fft, 3)  # no cache: the occupancy model's tiles
+    monkeypatch.setenv("EVP_TUNE", "0")
+    before = _rows(fft, 3)  # the occupancy model's tiles
+    monkeypatch.delenv("EVP_TUNE")
     cache = tmp_path / "tiles" / "fftw_wisdom.save"
     tune_cache(cache)
     try:
@@ -37,7 +40,7 @@ def test_tuned_tiles_are_cached_and_change_nothing(tmp_path):
         assert len(lines) >= 3 and all(l.startswith("evp-tile ") for l in lines)
         assert {int(l.split()[1]) for l in lines} == {0, 1, 2}  # x forward, y, z with the Green operator
         again = _rows(fft, 3)
-        assert cache.read_text().splitlines() == lines  # read, not timed again
+        assert cache.read_text().splitlines() == lines  # known: not timed again
     finally:
         tune_cache(None)
     keep = [c for c in range(before.shape[1]) if c != 4]
