@@ -17,7 +17,9 @@ namespace evp {
 
 class Batch;
 
-Batch* batch_create();  // on the current device
+Batch* batch_create(int priority = 0);  // on the current device; priority: its stream's CUDA priority
+// The highest stream priority of the device (numerically smallest); *lowest gets the lowest.
+int batch_priority_range(int* lowest);
 void batch_destroy(Batch* b);
 // Opens a member (deck already parsed into dk, moved from); returns its slot, or -1 with err set.
 int batch_add(Batch* b, Deck&& dk, const std::string& fft_in, const std::string& out_dir, int mix, int modal, int flags,
@@ -25,6 +27,13 @@ int batch_add(Batch* b, Deck&& dk, const std::string& fft_in, const std::string&
 // Runs `rounds` rounds (each: a few iterations of every running member and the host side of
 // their events).  Returns the number of members still running.
 int batch_step(Batch* b, int rounds);
+// The same round in three calls, so that one host thread can keep several batches (on
+// streams of different priority) busy: batch_launch queues a round (false when no member
+// runs), batch_ready says whether its iterations have run, batch_finish does the host side
+// of the round's events and returns the number of members still running.
+bool batch_launch(Batch* b);
+bool batch_ready(Batch* b);
+int batch_finish(Batch* b);
 // 0 running, 1 finished (status in *status: 0 ok or a code), -1 no such slot.
 int batch_slot(Batch* b, int slot, int* status, evp_report* rep, std::string* err);
 void batch_remove(Batch* b, int slot);  // releases a finished slot's device memory

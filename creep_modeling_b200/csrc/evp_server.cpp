@@ -3,13 +3,14 @@
 // The reference answers each request with a new solver process
 // (utils/run.py:169-196; calibrate.py runs two or three at once,
 // calibrate.py:1053-1057).  Here one process keeps a server: requests are parsed on
-// the submitting thread and queue; one engine thread owns a Batch (evp_batch.h) on
-// the server's GPU.  Between rounds of batched iterations it admits queued requests
+// the submitting thread and queue; one engine thread owns two Batches (evp_batch.h)
+// on the server's GPU.  Between rounds of batched iterations it admits queued requests
 // while their device-memory estimates fit the budget (the smallest remaining work
-// first: voxels times increments), so requests that arrive while others run join the
+// first: voxels times increments), so requests that arrive while others run join a
 // running batch as soon as memory and a slot free up, and their work shares the
 // launches of every solve already on the device.  Finished solves (their files
-// written) leave the batch at once.
+// written) leave the batch at once.  Two batches run side by side: small grids on a
+// stream of the highest priority, the others on the lowest, each with its own rounds.
 #include "../../include/evp.h"
 #include "evp_batch.h"
 #include "evp_deck.h"
@@ -68,12 +69,17 @@ double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::dura
 
 }  // namespace
 
+// Solves of at most this many voxels (40^3) run in the small lane: a batch on a stream of the
+// device's highest priority, so their short rounds get SMs ahead of the large lane's long ones
+// and a small request's latency does not follow the round time of the largest solves.
+constexpr long long kSmallLaneVoxels = 40LL * 40 * 40;
+
 struct evp_server {
     std::mutex m;
     std::condition_variable cv;  // any change of queue, admission or completion
     std::deque<unsigned long long> queue;
     std::map<unsigned long long, Request> reqs;
-    std::map<int, unsigned long long> slot_req;  // batch slot -> request
+    std::map<std::pair<int, int>, unsigned long long> slot_req;  // (lane, batch slot) -> request
     std::thread engine;
     unsigned long long budget = 0, used = 0, next_id = 1;
     int max_inflight = 16, inflight = 0, device = 0;
@@ -107,17 +113,23 @@ struct evp_server {
 
     void engine_loop() {
         cudaSetDevice(device);
-        std::unique_ptr<evp::Batch, void (*)(evp::Batch*)> batch(nullptr, evp::batch_destroy);
+        using BatchPtr = std::unique_ptr<evp::Batch, void (*)(evp::Batch*)>;
+        BatchPtr lane[2] = {BatchPtr(nullptr, evp::batch_destroy), BatchPtr(nullptr, evp::batch_destroy)};
         try {
-            batch.reset(evp::batch_create());
+            int lowest = 0;
+            const int highest = evp::batch_priority_range(&lowest);
+            lane[0].reset(evp::batch_create(highest));
+            lane[1].reset(evp::batch_create(lowest));
         } catch (std::exception& e) {
             std::lock_guard<std::mutex> lk(m);
             fatal = e.what();
         }
+        const bool ok = lane[0] && lane[1];
+        bool pending[2] = {false, false};
         std::unique_lock<std::mutex> lk(m);
         while (true) {
             // admission: smallest remaining work first, while slots and memory allow
-            while (batch && inflight < max_inflight && !queue.empty()) {
+            while (ok && inflight < max_inflight && !queue.empty()) {
                 const unsigned long long id = pick();
                 if (id == 0) break;
                 for (auto it = queue.begin(); it != queue.end(); ++it)
@@ -134,11 +146,12 @@ struct evp_server {
                 const std::string fft = r.fft, out = r.out;
                 const int mix = r.mix, modal = r.modal, flags = r.flags;
                 const double dl = r.deadline_s;
+                const int l = (long long)r.n1 * r.n2 * r.n3 <= kSmallLaneVoxels ? 0 : 1;
                 lk.unlock();
                 std::string err;
                 int slot = -1;
                 try {
-                    slot = evp::batch_add(batch.get(), std::move(*dk), fft, out, mix, modal, flags, dl, err);
+                    slot = evp::batch_add(lane[l].get(), std::move(*dk), fft, out, mix, modal, flags, dl, err);
                 } catch (std::exception& e) {
                     err = e.what();
                 }
@@ -146,19 +159,19 @@ struct evp_server {
                 Request& q = reqs[id];
                 int status = 0;
                 evp_report rep{};
-                const int st = slot >= 0 ? evp::batch_slot(batch.get(), slot, &status, &rep, &err) : 1;
+                const int st = slot >= 0 ? evp::batch_slot(lane[l].get(), slot, &status, &rep, &err) : 1;
                 if (slot < 0) status = -6;
                 if (st == 1) {  // failed at start-up (or a deck without steps)
                     complete(q, status, err, rep.macrosteps, rep.voxel_iters);
-                    if (slot >= 0) evp::batch_remove(batch.get(), slot);
+                    if (slot >= 0) evp::batch_remove(lane[l].get(), slot);
                     used -= q.foot;
                     inflight--;
                     cv.notify_all();
                 } else {
-                    slot_req[slot] = id;
+                    slot_req[{l, slot}] = id;
                 }
             }
-            if (!batch) {  // no device: fail what is queued
+            if (!ok) {  // no device: fail what is queued
                 for (auto id : queue) complete(reqs[id], -6, fatal, 0, 0);
                 queue.clear();
                 cv.notify_all();
@@ -172,18 +185,32 @@ struct evp_server {
                 continue;
             }
             lk.unlock();
+            // keep a round queued on each lane that has members; finish whichever is done first
             std::string step_err;
             try {
-                evp::batch_step(batch.get(), 1);
+                for (int l = 0; l < 2; l++)
+                    if (!pending[l]) pending[l] = evp::batch_launch(lane[l].get());
+                bool any = false;
+                while (!any && (pending[0] || pending[1])) {
+                    for (int l = 0; l < 2; l++)
+                        if (pending[l] && evp::batch_ready(lane[l].get())) {
+                            evp::batch_finish(lane[l].get());
+                            pending[l] = false;
+                            any = true;
+                        }
+                    if (!any) std::this_thread::sleep_for(std::chrono::microseconds(20));
+                }
             } catch (std::exception& e) {
                 step_err = e.what();
+                pending[0] = pending[1] = false;
             }
             lk.lock();
             for (auto it = slot_req.begin(); it != slot_req.end();) {
                 int status = 0;
                 evp_report rep{};
                 std::string err;
-                const int st = evp::batch_slot(batch.get(), it->first, &status, &rep, &err);
+                evp::Batch* b = lane[it->first.first].get();
+                const int st = evp::batch_slot(b, it->first.second, &status, &rep, &err);
                 if (st == 1 || !step_err.empty()) {
                     Request& q = reqs[it->second];
                     if (st != 1) {
@@ -191,7 +218,7 @@ struct evp_server {
                         err = step_err;
                     }
                     complete(q, status, err, rep.macrosteps, rep.voxel_iters);
-                    evp::batch_remove(batch.get(), it->first);
+                    if (st == 1 || !pending[it->first.first]) evp::batch_remove(b, it->first.second);
                     used -= q.foot;
                     inflight--;
                     it = slot_req.erase(it);

@@ -1272,11 +1272,17 @@ public:
     bool dirty = false;
     int check_every = 4;
 
-    Batch() {
-        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t round_ev = nullptr;  // recorded after a launched round's iterations
+    bool in_round = false;
+
+    // priority: CUDA stream priority of the batch's stream (0 default; lower numbers run first)
+    explicit Batch(int priority = 0) {
+        CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
+        CK(cudaEventCreateWithFlags(&round_ev, cudaEventDisableTiming));
         eng.reset(new Engine(st));
     }
     ~Batch() {
+        if (round_ev) cudaEventDestroy(round_ev);
         eng.reset();
         for (auto& sl : slots) sl.s.reset();
         if (st) {
@@ -1354,16 +1360,30 @@ public:
         dirty = false;
     }
 
-    // one round: check_every iterations of every running member, then the host side of their events
-    void round() {
+    // One round: check_every iterations of every running member (launch_round, asynchronous),
+    // then, once they have run (round_done), the host side of their events (finish_round).
+    bool launch_round() {
+        if (in_round) return true;
         if (dirty) rebuild();
-        if (members.empty()) return;
+        if (members.empty()) return false;
         eng->launch(check_every, nullptr);
+        CK(cudaEventRecord(round_ev, st));
+        in_round = true;
+        return true;
+    }
+    bool round_done() const { return !in_round || cudaEventQuery(round_ev) != cudaErrorNotReady; }
+    void round() {
+        if (launch_round()) finish_round();
+    }
+    void finish_round() {
+        if (!in_round) return;
+        in_round = false;
         const int per_iter = eng->launches_per_iteration();
         const int* ev = eng->read_events();
         std::vector<int> ended;  // member positions whose increment iteration is over
         for (int i = 0; i < (int)members.size(); i++) {
             const int id = members[i];
+            if (!slots[id].s || slots[id].state != 0) continue;
             Solver& s = *slots[id].s;
             s.launches += (long long)check_every * per_iter;
             try {
@@ -1412,7 +1432,20 @@ public:
     }
 };
 
-Batch* batch_create() { return new Batch(); }
+Batch* batch_create(int priority) { return new Batch(priority); }
+bool batch_launch(Batch* b) { return b->launch_round(); }
+bool batch_ready(Batch* b) { return b->round_done(); }
+int batch_finish(Batch* b) {
+    b->finish_round();
+    if (b->dirty) b->rebuild();
+    return b->running();
+}
+int batch_priority_range(int* lowest) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (lowest) *lowest = lo;
+    return hi;  // the highest priority (numerically smallest)
+}
 void batch_destroy(Batch* b) { delete b; }
 int batch_add(Batch* b, Deck&& dk, const std::string& fft_in, const std::string& out_dir, int mix, int modal, int flags,
               double deadline_s, std::string& err) {
@@ -1592,7 +1625,7 @@ int evp_batch_open(evp_batch** out) {
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return fail("no CUDA device available", -6);
     try {
         evp_batch* h = new evp_batch();
-        h->b = evp::batch_create();
+        h->b = evp::batch_create(0);
         *out = h;
     } catch (SolveError& e) {
         return fail(e.what(), e.code);

@@ -166,16 +166,18 @@ int evp_solve_files(int n, const char* const* fft_in, const char* const* out_dir
  * A server keeps every admitted solve's fields on the device until the solve
  * ends and writes the same files as evp_solve_file.  evp_submit reads the deck
  * on the caller's thread (a deck error makes the request done at once with its
- * status); requests then queue.  One engine thread runs all admitted solves as
- * one batch (the evp_batch_* form: every equilibrium iteration is one launch per
- * pass over all of them, whatever their grid sizes).  Between rounds of a few
+ * status); requests then queue.  One engine thread runs the admitted solves as
+ * batches (the evp_batch_* form: every equilibrium iteration is one launch per
+ * pass over all of a batch's solves, whatever their grid sizes).  Between rounds of a few
  * iterations it admits queued requests, the one with the least work (voxels x
  * increments) first, while fewer than max_inflight solves run and the request's
  * estimated device footprint fits the budget beside the running ones; a request
  * larger than the whole budget runs alone.  So requests that arrive while others
- * are on the GPU join the running batch as soon as a slot and memory free up
- * (continuous batching), and a solve that finishes leaves it at once.  A solve's
- * results do not depend on what else runs beside it. */
+ * are on the GPU join a running batch as soon as a slot and memory free up
+ * (continuous batching), and a solve that finishes leaves it at once.  Solves of
+ * at most 40^3 voxels run in a second batch on a stream of the highest priority,
+ * with rounds of their own, so small requests are not paced by the largest ones.
+ * A solve's results do not depend on what else runs beside it. */
 typedef struct evp_server evp_server;
 
 typedef struct evp_status {
