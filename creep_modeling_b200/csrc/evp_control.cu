@@ -121,6 +121,7 @@ __device__ void control_one(IterCtl& c, const double* red, int err) {
     if (err & 1) return stop(c, -3, 1);
     if (err & 2) return stop(c, -4, 2);
     if (err & 4) return stop(c, -3, 4);
+    if (err & 8) return stop(c, -6, 64);
     const double* cr = red + OFF_CORR;
     for (int k = 0; k < 9; k++) {
         c.velgradavg[k] = cr[k];

@@ -101,7 +101,8 @@ struct Dev {
     // updates, [4] voxels, [5] warp passes of the Newton-step loop
     unsigned long long* nstats;
     unsigned int *counters;
-    int *err;  // error word: bit 0 singular matrix, bit 1 non-finite Newton result, bit 2 form_G failure
+    int *err;  // error word: bit 0 singular matrix, bit 1 non-finite Newton result, bit 2 form_G failure,
+               // bit 3 a TMA bulk copy that did not complete within its bounded wait
     const PhaseDev *ph;
     int nph;
 };

@@ -314,11 +314,56 @@ __device__ __forceinline__ void body_fft_y(const Dev& d, const FftPlan1D& pl, in
     const int n1h = d.n1h, n2 = d.n2, n3 = d.n3;
     const int kx0 = vb.x * T, k3 = vb.y, c = vb.z;
     CT* base = reinterpret_cast<CT*>(d.spec) + ((long long)c * n3 + k3) * n2 * n1h;
-    for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
-        const int t = idx % T, j = idx / T, kx = kx0 + t;
-        s[j * T + t] = (kx < n1h) ? base[(long long)j * n1h + kx] : mk<CT>(0, 0);
+    if constexpr (sizeof(CT) == 16) {
+        // FP64 spectrum: the block's pencils arrive by TMA bulk copies, one per y row (the row's
+        // valid columns, ncol x 16 bytes, 16-byte aligned at both ends), completing on an mbarrier;
+        // columns past the spectrum's edge are zeroed by ordinary stores (disjoint addresses)
+        __shared__ __align__(8) unsigned long long bar;
+        const int ncol = min(T, n1h - kx0);
+        const unsigned sbar = (unsigned)__cvta_generic_to_shared(&bar);
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned bytes = (unsigned)(n2 * ncol * 16);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar), "r"(bytes) : "memory");
+            for (int j = 0; j < n2; j++) {
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(s + (size_t)j * T);
+                const CT* src = base + (long long)j * n1h + kx0;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                    "l"(src), "r"((unsigned)(ncol * 16)), "r"(sbar)
+                    : "memory");
+            }
+        }
+        for (int idx = threadIdx.x; idx < (T - ncol) * n2; idx += blockDim.x) {
+            const int t = ncol + idx % (T - ncol), j = idx / (T - ncol);
+            s[j * T + t] = mk<CT>(0, 0);
+        }
+        // bounded wait for the copies' bytes (each try_wait suspends for a while before it fails)
+        unsigned done = 0;
+        for (long tries = 0; !done; tries++) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(sbar)
+                : "memory");
+            if (!done && tries > (1L << 20)) {
+                atomicOr(d.err, 8);  // the copies never completed: the solve stops with an error
+                break;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(sbar) : "memory");
+    } else {
+        for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
+            const int t = idx % T, j = idx / T, kx = kx0 + t;
+            s[j * T + t] = (kx < n1h) ? base[(long long)j * n1h + kx] : mk<CT>(0, 0);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     fft_run<INV, RS, CT>(s, T, T, pl, twid<CT>(d, 2));
     for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
         const int t = idx % T, j = idx / T, kx = kx0 + t;

@@ -233,6 +233,7 @@ public:
         if (*h_err & 1) throw SolveError("singular matrix in a voxel operator (lu_inverse / lu_eqsystem)", -3);
         if (*h_err & 2) throw SolveError("non-finite stress in the local Newton solve", -4);
         if (*h_err & 4) throw SolveError("form_G failed (singular acoustic tensor or complex D operator)", -3);
+        if (*h_err & 8) throw SolveError("a bulk copy into shared memory did not complete", -6);
     }
     void fetch_red() {
         fetch_red_async();
@@ -652,6 +653,7 @@ public:
         if (bits & 8) return "ERRE/ERRS negative -> convergence failed!";
         if (bits & 16) return "Failed system solve in lu_eqsystem (state_6x6_evpsc)";
         if (bits & 32) return "equilibrium iteration did not converge";
+        if (bits & 64) return "a bulk copy into shared memory did not complete";
         return "equilibrium iteration failed";
     }
 
