@@ -307,6 +307,49 @@ __global__ void __launch_bounds__(256, 2) k_fft_x_fwd(Dev d, FftPlan1D pl, int G
 }
 
 // ---------------------------------------------------------------- y (C2C)
+// TMA staging of pencils: nrows rows of ncol FP64 complex values (16 bytes each, so both
+// ends of every row are 16-byte aligned), row r from global src(r) to shared dst(r), by bulk
+// copies that complete on one mbarrier.  Thread 0 posts the expected byte count, then the 32
+// lanes of warp 0 issue the rows; every thread waits for the bytes with a bounded wait (each
+// try_wait suspends for a while before it fails; past the bound the error word gets bit 3 and
+// the solve stops).  Callers zero the columns past the spectrum's edge with ordinary stores.
+template <class SrcF, class DstF>
+__device__ __forceinline__ void tma_rows(int nrows, int ncol, SrcF src, DstF dst, int* err) {
+    __shared__ __align__(8) unsigned long long bar;
+    const unsigned sbar = (unsigned)__cvta_generic_to_shared(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) {
+            const unsigned bytes = (unsigned)(nrows * ncol * 16);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar), "r"(bytes) : "memory");
+        }
+        __syncwarp();
+        for (int r = threadIdx.x; r < nrows; r += 32) {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst(r));
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+                         "l"(src(r)), "r"((unsigned)(ncol * 16)), "r"(sbar)
+                         : "memory");
+        }
+    }
+    unsigned done = 0;
+    for (long tries = 0; !done; tries++) {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(sbar)
+                     : "memory");
+        if (!done && tries > (1L << 20)) {
+            atomicOr(err, 8);
+            break;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(sbar) : "memory");
+}
+
 template <bool INV, int RS, class CT>
 __device__ __forceinline__ void body_fft_y(const Dev& d, const FftPlan1D& pl, int T, const VB& vb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -315,48 +358,14 @@ __device__ __forceinline__ void body_fft_y(const Dev& d, const FftPlan1D& pl, in
     const int kx0 = vb.x * T, k3 = vb.y, c = vb.z;
     CT* base = reinterpret_cast<CT*>(d.spec) + ((long long)c * n3 + k3) * n2 * n1h;
     if constexpr (sizeof(CT) == 16) {
-        // FP64 spectrum: the block's pencils arrive by TMA bulk copies, one per y row (the row's
-        // valid columns, ncol x 16 bytes, 16-byte aligned at both ends), completing on an mbarrier;
-        // columns past the spectrum's edge are zeroed by ordinary stores (disjoint addresses)
-        __shared__ __align__(8) unsigned long long bar;
+        // FP64 spectrum: the block's pencils arrive by TMA bulk copies, one per y row (its valid columns)
         const int ncol = min(T, n1h - kx0);
-        const unsigned sbar = (unsigned)__cvta_generic_to_shared(&bar);
-        if (threadIdx.x == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbar) : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const unsigned bytes = (unsigned)(n2 * ncol * 16);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar), "r"(bytes) : "memory");
-            for (int j = 0; j < n2; j++) {
-                const unsigned dst = (unsigned)__cvta_generic_to_shared(s + (size_t)j * T);
-                const CT* src = base + (long long)j * n1h + kx0;
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                    "l"(src), "r"((unsigned)(ncol * 16)), "r"(sbar)
-                    : "memory");
-            }
-        }
         for (int idx = threadIdx.x; idx < (T - ncol) * n2; idx += blockDim.x) {
             const int t = ncol + idx % (T - ncol), j = idx / (T - ncol);
             s[j * T + t] = mk<CT>(0, 0);
         }
-        // bounded wait for the copies' bytes (each try_wait suspends for a while before it fails)
-        unsigned done = 0;
-        for (long tries = 0; !done; tries++) {
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                : "=r"(done)
-                : "r"(sbar)
-                : "memory");
-            if (!done && tries > (1L << 20)) {
-                atomicOr(d.err, 8);  // the copies never completed: the solve stops with an error
-                break;
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(sbar) : "memory");
+        tma_rows(n2, ncol, [&](int j) { return base + (long long)j * n1h + kx0; }, [&](int j) { return s + (size_t)j * T; },
+                 d.err);
     } else {
         for (int idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
             const int t = idx % T, j = idx / T, kx = kx0 + t;
@@ -412,11 +421,22 @@ __device__ __forceinline__ void body_fft_z_green(const Dev& d, const FftPlan1D& 
     const int P = 9 * T;
     for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = (Re)c0g[i]; s0[i] = (Re)s0g[i]; }
     const long long plane = (long long)n2 * n1h;
-    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
-        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
-        s[k3 * P + c * T + t] = (kx < n1h) ? spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : mk<CT>(0, 0);
+    if constexpr (sizeof(CT) == 16) {
+        // FP64 spectrum: one TMA bulk copy per (component, z) row of the block's kx range
+        const int ncol = min(T, n1h - kx0);
+        for (int idx = threadIdx.x; idx < (T - ncol) * 9 * n3; idx += blockDim.x) {
+            const int t = ncol + idx % (T - ncol), r = idx / (T - ncol), c = r % 9, k3 = r / 9;
+            s[k3 * P + c * T + t] = mk<CT>(0, 0);
+        }
+        tma_rows(9 * n3, ncol, [&](int r) { return spec + ((long long)(r % 9) * n3 + r / 9) * plane + (long long)j * n1h + kx0; },
+                 [&](int r) { return s + (size_t)(r / 9) * P + (r % 9) * T; }, d.err);
+    } else {
+        for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+            const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+            s[k3 * P + c * T + t] = (kx < n1h) ? spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : mk<CT>(0, 0);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     fft_run<false, RS, CT>(s, P, P, pl, twid<CT>(d, 3));
     const bool nyq_y = (n2 % 2 == 0 && j == n2 / 2);
     const Re xiy = (Re)xi_of(j, n2);
