@@ -421,22 +421,13 @@ __device__ __forceinline__ void body_fft_z_green(const Dev& d, const FftPlan1D& 
     const int P = 9 * T;
     for (int i = threadIdx.x; i < 81; i += blockDim.x) { c0[i] = (Re)c0g[i]; s0[i] = (Re)s0g[i]; }
     const long long plane = (long long)n2 * n1h;
-    if constexpr (sizeof(CT) == 16) {
-        // FP64 spectrum: one TMA bulk copy per (component, z) row of the block's kx range
-        const int ncol = min(T, n1h - kx0);
-        for (int idx = threadIdx.x; idx < (T - ncol) * 9 * n3; idx += blockDim.x) {
-            const int t = ncol + idx % (T - ncol), r = idx / (T - ncol), c = r % 9, k3 = r / 9;
-            s[k3 * P + c * T + t] = mk<CT>(0, 0);
-        }
-        tma_rows(9 * n3, ncol, [&](int r) { return spec + ((long long)(r % 9) * n3 + r / 9) * plane + (long long)j * n1h + kx0; },
-                 [&](int r) { return s + (size_t)(r / 9) * P + (r % 9) * T; }, d.err);
-    } else {
-        for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
-            const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
-            s[k3 * P + c * T + t] = (kx < n1h) ? spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : mk<CT>(0, 0);
-        }
-        __syncthreads();
+    // ordinary loads: the block's rows are short (T complex values per component and z), which
+    // suits TMA bulk copies badly (measured: 43 -> 68 us per 64^3 launch with one copy per row)
+    for (int idx = threadIdx.x; idx < P * n3; idx += blockDim.x) {
+        const int t = idx % T, r = idx / T, c = r % 9, k3 = r / 9, kx = kx0 + t;
+        s[k3 * P + c * T + t] = (kx < n1h) ? spec[((long long)c * n3 + k3) * plane + (long long)j * n1h + kx] : mk<CT>(0, 0);
     }
+    __syncthreads();
     fft_run<false, RS, CT>(s, P, P, pl, twid<CT>(d, 3));
     const bool nyq_y = (n2 % 2 == 0 && j == n2 / 2);
     const Re xiy = (Re)xi_of(j, n2);
