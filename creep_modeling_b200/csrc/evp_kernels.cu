@@ -366,15 +366,26 @@ __global__ void __launch_bounds__(kBlock, 2) k_prologue(Dev d, const double* __r
         basis_T(F, TF);
         congruence6(TF, c0b, 1.0 / detF, c66);
         for (int c = 0; c < 36; c++) d.c066mod[c * N + v] = c66[c];
-        {  // its inverse, for the symmetric form of the local Newton system
-            double ci[36];
+        // its inverse, for the symmetric form of the local Newton system (in place: c066mod is stored)
+        if (inv_unrolled<6>(c66) != 0 && !gas) set_err(d.err, 1);
 #pragma unroll
-            for (int c = 0; c < 36; c++) ci[c] = c66[c];
-            if (inv_unrolled<6>(ci) != 0 && !gas) set_err(d.err, 1);
+        for (int c = 0; c < 36; c++) d.c066inv[c * N + v] = c66[c];
+    }
+}
+// calc_c066mod_Goperr066mod, the modified augmented Lagrangian part (various_functions.f90:866-900):
+// cG = C~ : Gamma~r with Gamma~r = sym(J Gamma^r(0) F^-1 F^-1), for --modal 1 only (a kernel of its
+// own, so that its 3x3x3x3 work arrays do not burden the common prologue's registers)
+__global__ void __launch_bounds__(kBlock, 2) k_prologue_modal(Dev d, const double* __restrict__ g0g) {
+    __shared__ double g0[81];
+    for (int i = threadIdx.x; i < 81; i += blockDim.x) g0[i] = g0g[i];
+    __syncthreads();
+    const long long N = d.N;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < N; v += (long long)gridDim.x * blockDim.x) {
+        const double detF = d.detF[v];
+        double c66[36];
 #pragma unroll
-            for (int c = 0; c < 36; c++) d.c066inv[c * N + v] = ci[c];
-        }
-        if (modal) {
+        for (int c = 0; c < 36; c++) c66[c] = d.c066mod[c * N + v];
+        {
             double Fi[9], g66[36], cm[81], cs[81];
             ld9(d.Finv, N, v, Fi);
             for (int ii = 0; ii < 3; ii++)
@@ -405,6 +416,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_prologue(Dev d, const double* __r
 }
 void launch_prologue(const Dev& d, const double* c0, const double* goperr0, int do_schmid, int modal, cudaStream_t st) {
     k_prologue<<<d.grid, kBlock, 0, st>>>(d, c0, goperr0, do_schmid, modal);
+    if (modal) k_prologue_modal<<<d.grid, kBlock, 0, st>>>(d, goperr0);
 }
 
 // ---------------------------------------------------------------- k_gas_compl
