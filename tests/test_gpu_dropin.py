@@ -3,7 +3,8 @@
 utils/run.py:169-196 (run_solver) launches the solver with
     set -o pipefail; EXE --nthreads n --in F --out D --fftw_save P --mix m --modal a | tee LOG;
 and then reads results.csv, diagnostics.csv and the VTK files it wrote.  Here
-the same command line runs creep_modeling_b200/LS-EVPFFT as a process, and
+that command line, recorded from the reference's own run_solver
+(tests/golden/make_run_solver_cmd.py), runs creep_modeling_b200/LS-EVPFFT as a process, and
 evp_solve_file runs the same deck in-process; both output directories must hold
 the oracle's files: same names, the CSV columns within the parity bar and every
 VTK number within 2e-8 of its block's largest magnitude (tests/test_gpu_files.py).
@@ -26,6 +27,7 @@ pytestmark = pytest.mark.gpu
 
 ROOT = Path(__file__).resolve().parents[1]
 EXE = ROOT / "creep_modeling_b200" / "LS-EVPFFT"
+GOLD = ROOT / "tests" / "golden"
 
 
 def _oracle_files(oracle_lib, fft, out, modal):
@@ -62,13 +64,18 @@ def deck(tmp_path):
 
 
 def test_executable_as_run_solver_launches_it(tmp_path, deck, oracle_lib):
+    """The command is the one the reference's run_solver builds (recorded from its own code in
+    tests/golden/run_solver_cmd.txt), with this repository's executable as SOLVER_EXE."""
     out, log = tmp_path / "evpfft_outputs", tmp_path / "output.txt"
-    cmd = (f"set -o pipefail; {EXE} --nthreads 4 --in {deck} --out {out} --fftw_save {tmp_path / 'fftw.save'} "
-           f"--mix 1 --modal 0 | tee {log}; ")
+    wisdom = tmp_path / "fftw" / "fftw_wisdom.save"
+    cmd = (GOLD / "run_solver_cmd.txt").read_text().strip()
+    for k, v in (("@EXE@", EXE), ("@FFT@", deck), ("@OUT@", out), ("@WISDOM@", wisdom), ("@LOG@", log)):
+        cmd = cmd.replace(k, str(v))
     env = {k: v for k, v in os.environ.items() if k != "EVP_SERVER_SOCKET"}
     r = subprocess.run(["bash", "-c", cmd], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert "MACROSTEPS=" in log.read_text()
+    assert wisdom.read_text().startswith("evp-tile ")  # --fftw_save named the FFT tile cache
     _oracle_files(oracle_lib, deck, tmp_path / "oracle", 0)
     _compare_dirs(out, tmp_path / "oracle")
 
