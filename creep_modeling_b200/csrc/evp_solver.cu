@@ -27,6 +27,7 @@
 #include <cstring>
 #include <ctime>
 #include <string>
+#include <thread>
 #include <vector>
 #include <sys/stat.h>
 
@@ -1060,6 +1061,31 @@ public:
         sync();
         return h;
     }
+    // Lines [0, n) of one VTK block, formatted by line(buffer, index) on several host threads in
+    // contiguous slices and written in order: the file is byte-identical to a serial write.
+    template <class Line>
+    static void emit_lines(FILE* f, long long n, Line&& line) {
+        const long long per = 16384;  // lines per slice (~1 MB of text)
+        const long long nslice = (n + per - 1) / per;
+        const int nthr = (int)std::max(1LL, std::min<long long>(nslice, std::max(1u, std::thread::hardware_concurrency())));
+        const long long wave = (long long)nthr;
+        std::vector<std::string> buf(nthr);
+        for (long long s0 = 0; s0 < nslice; s0 += wave) {
+            const int m = (int)std::min(wave, nslice - s0);
+            auto work = [&](int t) {
+                std::string& o = buf[t];
+                o.clear();
+                const long long a = (s0 + t) * per, b = std::min(n, a + per);
+                for (long long i = a; i < b; i++) line(o, i);
+            };
+            std::vector<std::thread> th;
+            for (int t = 1; t < m; t++) th.emplace_back(work, t);
+            work(0);
+            for (auto& x : th) x.join();
+            for (int t = 0; t < m; t++) std::fwrite(buf[t].data(), 1, buf[t].size(), f);
+        }
+    }
+
     void write_vtk(int istp) {  // write_vtk_cell (IO_functions.f90:945-1235)
         const long long N = d.N;
         const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
@@ -1077,100 +1103,89 @@ public:
         std::string path = outdir + "/" + name;
         FILE* f = std::fopen(path.c_str(), "w");
         if (!f) throw SolveError("ioerr in writevtk", -5);
-        std::string o;
-        o.reserve(1 << 20);
         char b[256];
-        o += "# vtk DataFile Version 3.0\nmicrostructure data\nASCII\nDATASET UNSTRUCTURED_GRID\n";
+        auto put = [&](const char* text) { std::fputs(text, f); };
+        put("# vtk DataFile Version 3.0\nmicrostructure data\nASCII\nDATASET UNSTRUCTURED_GRID\n");
         const long long nn1 = n1 + 1, nn2 = n2 + 1;
-        auto nid = [&](int i, int j, int k) { return (long long)i + nn1 * ((long long)j + nn2 * (long long)k); };
-        auto flush = [&]() { std::fwrite(o.data(), 1, o.size(), f); o.clear(); };
+        auto nid = [&](long long i, long long j, long long k) { return i + nn1 * (j + nn2 * k); };
+        auto point = [&](std::string& o, long long q) {  // node q in (i, j, k) order, i fastest
+            put_e18(o, xn[3 * q]);
+            put_e18(o, xn[3 * q + 1]);
+            put_e18(o, xn[3 * q + 2]);
+            o += '\n';
+        };
         long long ncell;
         if (n3 == 1) {
             std::snprintf(b, sizeof(b), "POINTS%10lld double\n", nn1 * nn2);
-            o += b;
-            for (int j = 0; j < n2 + 1; j++)
-                for (int i = 0; i < n1 + 1; i++) {
-                    long long q = 3 * nid(i, j, 0);
-                    put_e18(o, xn[q]); put_e18(o, xn[q + 1]); put_e18(o, xn[q + 2]);
-                    o += '\n';
-                }
+            put(b);
+            emit_lines(f, nn1 * nn2, point);
             ncell = (long long)n1 * n2;
             std::snprintf(b, sizeof(b), "CELLS%10lld%10lld\n", ncell, ncell * 5);
-            o += b;
-            for (int j = 0; j < n2; j++)
-                for (int i = 0; i < n1; i++) {
-                    std::snprintf(b, sizeof(b), "%10d%10lld%10lld%10lld%10lld\n", 4, nid(i, j, 0), nid(i + 1, j, 0), nid(i, j + 1, 0), nid(i + 1, j + 1, 0));
-                    o += b;
-                }
+            put(b);
+            emit_lines(f, ncell, [&](std::string& o, long long c) {
+                char t[128];
+                const long long i = c % n1, j = c / n1;
+                std::snprintf(t, sizeof(t), "%10d%10lld%10lld%10lld%10lld\n", 4, nid(i, j, 0), nid(i + 1, j, 0), nid(i, j + 1, 0),
+                              nid(i + 1, j + 1, 0));
+                o += t;
+            });
             std::snprintf(b, sizeof(b), "CELL_TYPES%10lld\n", ncell);
-            o += b;
-            for (long long c = 0; c < ncell; c++) o += "    8\n";
+            put(b);
+            emit_lines(f, ncell, [](std::string& o, long long) { o += "    8\n"; });
         } else {
             std::snprintf(b, sizeof(b), "POINTS%10lld double\n", nn1 * nn2 * (n3 + 1));
-            o += b;
-            for (int k = 0; k < n3 + 1; k++)
-                for (int j = 0; j < n2 + 1; j++)
-                    for (int i = 0; i < n1 + 1; i++) {
-                        long long q = 3 * nid(i, j, k);
-                        put_e18(o, xn[q]); put_e18(o, xn[q + 1]); put_e18(o, xn[q + 2]);
-                        o += '\n';
-                        if (o.size() > (1 << 20)) flush();
-                    }
+            put(b);
+            emit_lines(f, nn1 * nn2 * (n3 + 1), point);
             ncell = N;
             std::snprintf(b, sizeof(b), "CELLS%10lld%10lld\n", ncell, ncell * 9);
-            o += b;
-            for (int k = 0; k < n3; k++)
-                for (int j = 0; j < n2; j++)
-                    for (int i = 0; i < n1; i++) {
-                        std::snprintf(b, sizeof(b), "%10d%10lld%10lld%10lld%10lld%10lld%10lld%10lld%10lld\n", 8, nid(i, j, k), nid(i + 1, j, k),
-                                      nid(i + 1, j + 1, k), nid(i, j + 1, k), nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1),
-                                      nid(i, j + 1, k + 1));
-                        o += b;
-                        if (o.size() > (1 << 20)) flush();
-                    }
+            put(b);
+            emit_lines(f, ncell, [&](std::string& o, long long c) {
+                char t[160];
+                const long long i = c % n1, j = (c / n1) % n2, k = c / ((long long)n1 * n2);
+                std::snprintf(t, sizeof(t), "%10d%10lld%10lld%10lld%10lld%10lld%10lld%10lld%10lld\n", 8, nid(i, j, k), nid(i + 1, j, k),
+                              nid(i + 1, j + 1, k), nid(i, j + 1, k), nid(i, j, k + 1), nid(i + 1, j, k + 1), nid(i + 1, j + 1, k + 1),
+                              nid(i, j + 1, k + 1));
+                o += t;
+            });
             std::snprintf(b, sizeof(b), "CELL_TYPES%10lld\n", ncell);
-            o += b;
-            for (long long c = 0; c < ncell; c++) o += "   12\n";
+            put(b);
+            emit_lines(f, ncell, [](std::string& o, long long) { o += "   12\n"; });
         }
         std::snprintf(b, sizeof(b), "CELL_DATA%10lld\nFIELD FieldData%10d\n", ncell, 11);
-        o += b;
+        put(b);
         const int ns = d.nsys;
         std::snprintf(b, sizeof(b), "gamdot%3d%10lld double\n", ns, ncell);
-        o += b;
-        for (long long v = 0; v < N; v++) {
-            for (int s = 0; s < ns; s++) put_e18(o, gd[s * N + v]);
+        put(b);
+        emit_lines(f, N, [&](std::string& o, long long v) {
+            for (int q = 0; q < ns; q++) put_e18(o, gd[q * N + v]);
             o += '\n';
-            if (o.size() > (1 << 20)) flush();
-        }
+        });
         auto scalar = [&](const char* nm, const std::vector<double>& a) {
             std::snprintf(b, sizeof(b), "%s%3d%10lld double\n", nm, 1, ncell);
-            o += b;
-            for (long long v = 0; v < N; v++) {
+            put(b);
+            emit_lines(f, N, [&](std::string& o, long long v) {
                 put_e18(o, a[v]);
                 o += '\n';
-                if (o.size() > (1 << 20)) flush();
-            }
+            });
         };
         auto tens9 = [&](const char* nm, const std::vector<double>& a) {  // column-major order
             std::snprintf(b, sizeof(b), "%s%3d%10lld double\n", nm, 9, ncell);
-            o += b;
-            for (long long v = 0; v < N; v++) {
+            put(b);
+            emit_lines(f, N, [&](std::string& o, long long v) {
                 for (int c = 0; c < 3; c++)
                     for (int r = 0; r < 3; r++) put_e18(o, a[(3 * r + c) * N + v]);
                 o += '\n';
-                if (o.size() > (1 << 20)) flush();
-            }
+            });
         };
         scalar("gamdot_acum", ga);
         tens9("def_grad_p", fp);
         std::snprintf(b, sizeof(b), "stress%3d%10lld double\n", 6, ncell);
-        o += b;
-        for (long long v = 0; v < N; v++) {
+        put(b);
+        emit_lines(f, N, [&](std::string& o, long long v) {
             put_e18(o, sg[0 * N + v]); put_e18(o, sg[1 * N + v]); put_e18(o, sg[2 * N + v]);
             put_e18(o, sg[5 * N + v]); put_e18(o, sg[3 * N + v]); put_e18(o, sg[4 * N + v]);
             o += '\n';
-            if (o.size() > (1 << 20)) flush();
-        }
+        });
         std::vector<double> svm(N);
         for (long long v = 0; v < N; v++) {
             double s6[6], t[9];
@@ -1182,22 +1197,21 @@ public:
         tens9("def_grad", F);
         scalar("det_def_grad", dF);
         std::snprintf(b, sizeof(b), "gr_id%3d%10lld int\n", 1, ncell);
-        o += b;
-        for (long long v = 0; v < N; v++) {
-            std::snprintf(b, sizeof(b), "%10d\n", dk.grain[v]);
-            o += b;
-            if (o.size() > (1 << 20)) flush();
-        }
+        put(b);
+        emit_lines(f, N, [&](std::string& o, long long v) {
+            char t[32];
+            std::snprintf(t, sizeof(t), "%10d\n", dk.grain[v]);
+            o += t;
+        });
         std::snprintf(b, sizeof(b), "ph_id%3d%10lld int\n", 1, ncell);
-        o += b;
-        for (long long v = 0; v < N; v++) {
-            std::snprintf(b, sizeof(b), "%10d\n", dk.phase_id[v]);
-            o += b;
-            if (o.size() > (1 << 20)) flush();
-        }
+        put(b);
+        emit_lines(f, N, [&](std::string& o, long long v) {
+            char t[32];
+            std::snprintf(t, sizeof(t), "%10d\n", dk.phase_id[v]);
+            o += t;
+        });
         scalar("epvm", ep);
         tens9("velgrad", vg);
-        flush();
         std::fclose(f);
     }
 
