@@ -17,36 +17,28 @@
 
 namespace evp {
 
-// state_6x6_evpsc (various_functions.f90:1638-1705): the VPSC-Voigt macroscopic
-// state with mixed strain-rate / stress components.  Returns 0, or 1 when the
-// 6x6 system is singular (lu_eqsystem failure).
-__device__ int state_6x6_dev(const int* idsim, double* dbar, const int* iscau, double* sbar, const double* xm,
-                             const double* devp0, double* scauchy, double* dsim) {
-    double profac[6], dbarv[6], sbarv[6], devp0v[6], aux6[6], aux6a[6], a4[81], xmv[36], a33[9], A[36];
+// state_6x6_evpsc (various_functions.f90:1638-1705): the VPSC-Voigt macroscopic state with mixed
+// strain-rate / stress components.  The system matrix and its LU factors are per-increment
+// constants (state_6x6_factor, on the host); here the right-hand side and the substitution.
+__device__ void state_6x6_dev(const IterCtl& c, double* dbar, double* sbar, const double* devp0, double* scauchy,
+                              double* dsim) {
+    double profac[6], dbarv[6], sbarv[6], devp0v[6], aux6[6], aux6a[6], a33[9];
     for (int i = 1; i <= 6; i++) profac[i - 1] = 1.0 + (i / 4);
     for (int i = 0; i < 6; i++) {
         dbarv[i] = dsim[3 * ijv_a(i) + ijv_b(i)];
         sbarv[i] = scauchy[3 * ijv_a(i) + ijv_b(i)];
     }
-    b66_to_t4(xm, a4);
-    for (int i = 0; i < 6; i++)
-        for (int j = 0; j < 6; j++) xmv[6 * i + j] = a4[(3 * ijv_a(i) + ijv_b(i)) * 9 + 3 * ijv_a(j) + ijv_b(j)];
     b6_to_t2(devp0, a33);
     for (int i = 0; i < 6; i++) devp0v[i] = a33[3 * ijv_a(i) + ijv_b(i)];
     for (int i = 0; i < 6; i++) aux6[i] = dbarv[i] - devp0v[i];
     for (int i = 0; i < 6; i++) {
-        aux6a[i] = -1.0 * idsim[i] * aux6[i];
-        for (int j = 0; j < 6; j++) {
-            aux6a[i] = aux6a[i] + xmv[6 * i + j] * iscau[j] * sbarv[j] * profac[j];
-            A[6 * i + j] = iscau[j] * (i == j ? 1 : 0) - idsim[j] * xmv[6 * i + j] * profac[j];
-        }
+        aux6a[i] = -1.0 * c.idsim[i] * aux6[i];
+        for (int j = 0; j < 6; j++) aux6a[i] = aux6a[i] + c.xmv[6 * i + j] * c.iscau[j] * sbarv[j] * profac[j];
     }
-    int piv[6];
-    if (lu_factor(A, 6, piv) != 0) return 1;
-    lu_solve(A, 6, piv, aux6a);
+    lu_solve(c.lu, 6, c.piv, aux6a);
     for (int i = 0; i < 6; i++) {
-        aux6[i] = idsim[i] * aux6[i] + iscau[i] * aux6a[i];
-        sbarv[i] = iscau[i] * sbarv[i] + idsim[i] * aux6a[i];
+        aux6[i] = c.idsim[i] * aux6[i] + c.iscau[i] * aux6a[i];
+        sbarv[i] = c.iscau[i] * sbarv[i] + c.idsim[i] * aux6a[i];
     }
     for (int i = 0; i < 6; i++) dbarv[i] = aux6[i] + devp0v[i];
     for (int i = 0; i < 6; i++) {
@@ -57,11 +49,10 @@ __device__ int state_6x6_dev(const int* idsim, double* dbar, const int* iscau, d
     }
     t2_to_b6(dsim, dbar);
     t2_to_b6(scauchy, sbar);
-    return 0;
 }
 
 // calc_velgradavg_corr tail (various_functions.f90:1575-1631) on the solid stress sum.
-__device__ int velgradavg_corr_dev(IterCtl& c, const double* sgsol6) {
+__device__ void velgradavg_corr_dev(IterCtl& c, const double* sgsol6) {
     s6_to_t2(sgsol6, c.sgavg);
     for (int k = 0; k < 9; k++) c.sgavgsol[k] = c.sgavg[k] / c.wphcsol;
     c.svmavg = vm_stress(c.sgavg);
@@ -72,18 +63,17 @@ __device__ int velgradavg_corr_dev(IterCtl& c, const double* sgsol6) {
         a33[3 * jj + ii] = c.iscau[i] * (c.scauchy[3 * jj + ii] - c.sgavg[3 * jj + ii]);
     }
     c.errsbc = frob3(a33);
-    double vsym[9], vasym[9], dbar[6], sbar[6], mev[36], devp0[6];
+    double vsym[9], vasym[9], dbar[6], sbar[6], devp0[6];
     sym33(c.velgradavg, vsym);
     antisym33(c.velgradavg, vasym);
     t2_to_b6(vsym, dbar);
     t2_to_b6(c.sgavg, sbar);
-    t4_to_b66(c.de_ds, mev);
     for (int i = 0; i < 6; i++) {
         double s = 0.0;
-        for (int j = 0; j < 6; j++) s += mev[6 * i + j] * sbar[j];
+        for (int j = 0; j < 6; j++) s += c.mev[6 * i + j] * sbar[j];
         devp0[i] = dbar[i] - s;
     }
-    if (state_6x6_dev(c.idsim, dbar, c.iscau, sbar, mev, devp0, c.scauchy, c.dsim) != 0) return 1;
+    state_6x6_dev(c, dbar, sbar, devp0, c.scauchy, c.dsim);
     double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int ii = 0; ii < 3; ii++)
         for (int jj = 0; jj < 3; jj++) {
@@ -103,7 +93,6 @@ __device__ int velgradavg_corr_dev(IterCtl& c, const double* sgsol6) {
             }
         }
     for (int k = 0; k < 9; k++) c.xinv.dvelgradavg[k] = (c.dsim[k] - vsym[k]) + (w[k] - vasym[k]);
-    return 0;
 }
 
 __device__ void stop(IterCtl& c, int event, int bits) {
@@ -142,7 +131,7 @@ __device__ void control_one(IterCtl& c, const double* red, int err) {
     if (erre < 0 || errs < 0) return stop(c, -4, 8);
     erre = sqrt(erre);
     errs = sqrt(errs);
-    if (velgradavg_corr_dev(c, nw + 2) != 0) return stop(c, -3, 16);
+    velgradavg_corr_dev(c, nw + 2);
     c.erre = erre / c.lvmavg;
     c.errs = errs / c.svmavg;
     c.errsbc = c.errsbc / c.svmavg;

@@ -158,7 +158,11 @@ struct IterCtl {
     double erre, errs, errsbc, svmavg, wphcsol, wphcgas;
     double hist[4];  // the last four error maxima of the FP32 iterations (ring)
     double velgradavg[9], velgradavggas[9], velgradavgsol[9], sgavg[9], sgavgsol[9];
-    double de_ds[81];
+    // per-increment constants of calc_velgradavg_corr / state_6x6_evpsc, formed on the host at the
+    // start of the increment: de_ds in the b-basis (mev), its Voigt form (xmv) and the LU factors
+    // and pivots of the mixed-BC system (they depend only on de_ds and the process's masks)
+    double mev[36], xmv[36], lu[36];
+    int piv[6], pad6[2];
     // boundary conditions of the current process (dsim and scauchy change every iteration)
     int iscau[6], idsim[6], iudot[9];
     double udot[9], dsim[9], scauchy[9];

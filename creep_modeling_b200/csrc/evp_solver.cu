@@ -591,7 +591,22 @@ public:
         c.wphcsol = wphcsol;
         c.wphcgas = wphcgas;
         std::memcpy(c.velgradavg, velgradavg, sizeof(velgradavg));
-        std::memcpy(c.de_ds, de_ds, sizeof(de_ds));
+        // the increment's constants of state_6x6_evpsc (various_functions.f90:1638-1705): de_ds in the
+        // b-basis, its Voigt form and the LU factors of the mixed-BC system, formed by the same
+        // functions the per-iteration tail used to call, so every bit is as before
+        {
+            double a4[81];
+            t4_to_b66(de_ds, c.mev);
+            b66_to_t4(c.mev, a4);
+            for (int i = 0; i < 6; i++)
+                for (int j = 0; j < 6; j++) c.xmv[6 * i + j] = a4[(3 * ijv_a(i) + ijv_b(i)) * 9 + 3 * ijv_a(j) + ijv_b(j)];
+            double profac[6];
+            for (int i = 1; i <= 6; i++) profac[i - 1] = 1.0 + (i / 4);
+            for (int i = 0; i < 6; i++)
+                for (int j = 0; j < 6; j++)
+                    c.lu[6 * i + j] = p.iscau[j] * (i == j ? 1 : 0) - p.idsim[j] * c.xmv[6 * i + j] * profac[j];
+            if (lu_factor(c.lu, 6, c.piv) != 0) throw SolveError("Failed system solve in lu_eqsystem (state_6x6_evpsc)", -3);
+        }
         for (int i = 0; i < 6; i++) {
             c.iscau[i] = p.iscau[i];
             c.idsim[i] = p.idsim[i];
@@ -652,7 +667,6 @@ public:
         if (bits & 2) return "non-finite stress in the local Newton solve";
         if (bits & 4) return "form_G failed (singular acoustic tensor or complex D operator)";
         if (bits & 8) return "ERRE/ERRS negative -> convergence failed!";
-        if (bits & 16) return "Failed system solve in lu_eqsystem (state_6x6_evpsc)";
         if (bits & 32) return "equilibrium iteration did not converge";
         if (bits & 64) return "a bulk copy into shared memory did not complete";
         return "equilibrium iteration failed";
