@@ -143,6 +143,21 @@ def dist_env():
     return ws, rank, local
 
 
+def aggregate_replicas(pg, seconds: float, voxel_iters: float, device) -> tuple[float, float]:
+    """Whole-job figures of N independent replicas (one solve per rank, no data exchange): the
+    slowest rank's device time and the voxel-iterations of all ranks.  pg is torch.distributed
+    (or None for one process); the two reductions run in the same order on every rank."""
+    if pg is None:
+        return float(seconds), float(voxel_iters)
+    import torch
+
+    t = torch.tensor([float(seconds), float(voxel_iters)], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(tmax[0]), float(t[1])
+
+
 def make_deck(root: Path, n: int, nsteps: int, ngrains: int) -> Path:
     from creep_modeling_b200 import decks
 
@@ -431,14 +446,7 @@ def main(argv=None) -> int:
     gpu_s = st1.gpu_s - st0.gpu_s
     vi = (st1.equilibrium_iters - st0.equilibrium_iters) * (n ** 3)
     iters = st1.equilibrium_iters - st0.equilibrium_iters
-    if pg:
-        t = torch.tensor([gpu_s, float(vi)], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        pg.all_reduce(tmax, op=pg.ReduceOp.MAX)
-        pg.all_reduce(t, op=pg.ReduceOp.SUM)
-        gpu_s_max, vi_tot = float(tmax[0]), float(t[1])
-    else:
-        gpu_s_max, vi_tot = gpu_s, float(vi)
+    gpu_s_max, vi_tot = aggregate_replicas(pg, gpu_s, vi, dev)
     value = vi_tot / gpu_s_max
 
     # 2. end to end through the C ABI on the same increments: a second solve of the same deck

@@ -94,3 +94,39 @@ def test_executable_reports_a_deck_error(tmp_path):
     r = subprocess.run([str(EXE), "--in", str(bad), "--out", str(tmp_path / "o")], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 1 and "[-1:" in r.stderr
+
+
+def test_run_solver_command_through_the_socket_server(tmp_path, deck, oracle_lib):
+    """The same recorded run.py command with EVP_SERVER_SOCKET set: the shim submits the deck to
+    a resident server (a real GPU Server behind the JSON socket) and returns when its files are
+    written; they must equal the oracle's as in the direct run."""
+    import threading
+    import time
+
+    from creep_modeling_b200.serve import Server, serve_socket, submit_via_socket
+
+    sock = str(tmp_path / "evp.sock")
+    stop = threading.Event()
+    with Server(0, 4) as srv:
+        th = threading.Thread(target=serve_socket, args=(sock, srv, stop), daemon=True)
+        th.start()
+        for _ in range(500):
+            if os.path.exists(sock):
+                break
+            time.sleep(0.01)
+        out, log = tmp_path / "served_outputs", tmp_path / "served.txt"
+        cmd = (GOLD / "run_solver_cmd.txt").read_text().strip()
+        for k, v in (("@EXE@", EXE), ("@FFT@", deck), ("@OUT@", out), ("@WISDOM@", tmp_path / "w.save"), ("@LOG@", log)):
+            cmd = cmd.replace(k, str(v))
+        env = dict(os.environ, EVP_SERVER_SOCKET=sock)
+        r = subprocess.run(["bash", "-c", cmd], env=env, capture_output=True, text=True, timeout=600)
+        stop.set()
+        try:  # wake the accept loop so that it sees the stop flag
+            submit_via_socket(sock, "x.in", "o")
+        except Exception:
+            pass
+        th.join(timeout=10)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "(served)" in log.read_text()
+    _oracle_files(oracle_lib, deck, tmp_path / "oracle", 0)
+    _compare_dirs(out, tmp_path / "oracle")
