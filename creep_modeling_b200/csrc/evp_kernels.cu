@@ -1367,21 +1367,24 @@ __device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& 
         const bool gasv = d.gas[v];
         const int phi = d.phase[v];
         // rows r of C~ and H0, q'_r and this lane's systems; no load waits on the gas flag or phase
-        double qp_r;
+        double qp_r, sgt_r, D_r, eth_r = 0.0;  // component r of sgt, of D and of eth: kept for the closing norms
         {
             double lamf[6], sgtf[6], a[9], b6[6], vs[9];
             ld6(d.sg, N, v, a);
             s6_to_b6(a, lamf);
             ld6(d.sgt, N, v, a);
             s6_to_b6(a, sgtf);
+            sgt_r = sel6(sgtf, r);
             ld9(d.velgrad, N, v, a);
             sym33(a, vs);
             t2_to_b6(vs, b6);
-            double De = sel6(b6, r);
+            D_r = sel6(b6, r);
+            double De = D_r;
             if (p.thermo) {
                 ld9(d.eth, N, v, a);
                 t2_to_b6(a, b6);
-                De = De - sel6(b6, r);
+                eth_r = sel6(b6, r);
+                De = De - eth_r;
             }
             double cl = 0.0, ss = 0.0;
 #pragma unroll
@@ -1644,22 +1647,7 @@ __device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& 
         }
         // |sg - lam|^2 at the final stress; |edot - D|^2 at the last evaluation, with
         // edot = edotp + S (sg - sgt) / dt + eth as elastic_strain_rate forms it
-        double sgf[6], epf[6], ee = 0.0, sgt_r, D_r, eth_r = 0.0;
-        {
-            double a[9], b6[6], vs[9];
-            ld6(d.sgt, N, v, a);
-            s6_to_b6(a, b6);
-            sgt_r = sel6(b6, r);
-            ld9(d.velgrad, N, v, a);
-            sym33(a, vs);
-            t2_to_b6(vs, b6);
-            D_r = sel6(b6, r);
-            if (p.thermo) {
-                ld9(d.eth, N, v, a);
-                t2_to_b6(a, b6);
-                eth_r = sel6(b6, r);
-            }
-        }
+        double sgf[6], epf[6], ee = 0.0;
         {
             double dsf[6];
             xgather(X, (SEV[0] - sgt_r) / p.tdot, dsf);
