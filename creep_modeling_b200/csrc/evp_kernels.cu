@@ -1589,12 +1589,21 @@ __device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& 
                 }
             }
             if (p.iuphard) {  // harden (various_functions.f90:1439-1491)
+                // the committed resistances and accumulated shear, loaded first so that their latency
+                // overlaps the group sums and the exchange below
+                const double gamma0 = d.gacumgr[v];
+                double cr[SPL][2];
+#pragma unroll
+                for (int k = 0; k < SPL; k++) {
+                    const int s = r + 6 * k;
+                    cr[k][0] = s < nsyst ? d.crss[(2 * s) * N + v] : 0.0;
+                    cr[k][1] = s < nsyst ? d.crss[(2 * s + 1) * N + v] : 0.0;
+                }
                 double dg = 0.0;
 #pragma unroll
                 for (int k = 0; k < SPL; k++)
                     if (r + 6 * k < nsyst) dg += fabs(GD[k]) * p.tdot;
                 const double deltgam = xsum(X, dg);
-                const double gamma0 = d.gacumgr[v];
                 const double gamma1 = gamma0 + deltgam;
                 // |slip rate| of the group's system 6k + q in exchange row k, column base + q
                 __syncwarp();
@@ -1626,8 +1635,8 @@ __device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& 
 #pragma unroll
                         for (int js = 0; js < 6 * SPL; js++)
                             if (js < nsyst) dtau = dtau + ph.hard[s * MS + js] * X.P[(js / 6) * kXStride + base + js % 6];
-                        tn[k][0] = d.crss[(2 * s) * N + v] + dtau * voce * p.tdot / deltgam;
-                        tn[k][1] = d.crss[(2 * s + 1) * N + v] + dtau * voce * p.tdot / deltgam;
+                        tn[k][0] = cr[k][0] + dtau * voce * p.tdot / deltgam;
+                        tn[k][1] = cr[k][1] + dtau * voce * p.tdot / deltgam;
                     }
                     const double d0 = TT[2 * k] - tn[k][0], d1 = TT[2 * k + 1] - tn[k][1];
                     e2 += d0 * d0 + d1 * d1;
@@ -1649,10 +1658,12 @@ __device__ __forceinline__ void body_newton6p(const Dev& d, const NewtonParams& 
         // edot = edotp + S (sg - sgt) / dt + eth as elastic_strain_rate forms it
         double sgf[6], epf[6], ee = 0.0;
         {
-            double dsf[6];
+            double srow[6], dsf[6];  // row r of S loaded before the exchange, to overlap its latency
+#pragma unroll
+            for (int j = 0; j < 6; j++) srow[j] = d.sg66[(6 * r + j) * N + v];
             xgather(X, (SEV[0] - sgt_r) / p.tdot, dsf);
 #pragma unroll
-            for (int j = 0; j < 6; j++) ee += d.sg66[(6 * r + j) * N + v] * dsf[j];
+            for (int j = 0; j < 6; j++) ee += srow[j] * dsf[j];
         }
         double edot_r = EPM[0] + ee;
         if (p.thermo) edot_r = edot_r + eth_r;
