@@ -285,12 +285,25 @@ def _curve_err(a, b) -> float:
     return err
 
 
+def _plain_solve(fft, out):
+    """One solve through the plain single-solve path (evp_open / evp_advance / evp_close, the
+    steps of evp_solve_file) writing results.csv and diagnostics.csv, as the batched and served
+    legs do; returns its report."""
+    from creep_modeling_b200 import solver as S
+
+    s = S.Solve(fft, out_dir=str(out), mix=1, modal=0, csv_only=True)
+    s.run()
+    rep = s.stats()
+    s.close()
+    return rep
+
+
 def batch_sample(k: int, nsteps: int) -> dict:
     """The calibration sweep (configuration 4: grids 16^3-64^3, tau0, n and theta0 drawn per solve, creep
     at 120 MPa) on its first k solves at the full increment count: all of them as one batch
-    (evp_solve_files) against one after the other through the plain path (evp_solve_file each, as the
-    reference's callers run one solver process per solve).  Same decks, same files; the batch members'
-    results.csv must equal the one-by-one ones."""
+    (evp_solve_files) against one after the other through the plain single-solve path (as the
+    reference's callers run one solver process per solve).  Same decks; both write results.csv and
+    diagnostics.csv only; the batch members' results.csv must equal the one-by-one ones."""
     from creep_modeling_b200 import decks
     from creep_modeling_b200 import solver as S
 
@@ -301,7 +314,7 @@ def batch_sample(k: int, nsteps: int) -> dict:
     reps = S.solve_files(ffts, [td / f"b{i}" for i in range(k)], mix=1, modal=0, csv_only=True)
     tb = time.perf_counter() - t0
     t0 = time.perf_counter()
-    seq = [S.run_solver(f, td / f"s{i}", mix=1, modal=0) for i, f in enumerate(ffts)]
+    seq = [_plain_solve(f, td / f"s{i}") for i, f in enumerate(ffts)]
     ts = time.perf_counter() - t0
     same = all(_curve_err(_curves(td / f"b{i}" / "results.csv"), _curves(td / f"s{i}" / "results.csv")) == 0.0
                for i in range(k))
@@ -320,8 +333,9 @@ def serving_stream(k: int, rate: float) -> dict:
     475/525/575, creep 80-220 MPa, 50-400 increments) on its first k requests at their full increment
     counts, arriving as a Poisson stream of `rate` per s.  Served: one resident server, mixed precision,
     every admitted solve in one batch (continuous batching); latency = arrival -> files written.
-    Plain: the FP64 path, one solve after the other in arrival order (evp_solve_file each, as the
-    reference's run.py runs one process per request), latency = arrival -> its solve's end.
+    Plain: the FP64 single-solve path, one solve after the other in arrival order (as the reference's
+    run.py runs one process per request), latency = arrival -> its solve's end.  Both write
+    results.csv and diagnostics.csv only.
     Error: largest curve difference of every served (mixed) result against its plain FP64 result."""
     import numpy as np
 
@@ -360,7 +374,7 @@ def serving_stream(k: int, rate: float) -> dict:
         if dt > 0:
             time.sleep(dt)
         try:
-            r = S.run_solver(f, td / f"p{i}", mix=1, modal=0)
+            r = _plain_solve(f, td / f"p{i}")
             vi += r.voxel_iters
             pok += 1
         except Exception:
