@@ -50,9 +50,9 @@ Engine::~Engine() {
 }
 
 void Engine::drop_graph() {
-    if (graph_) cudaGraphExecDestroy(graph_);
-    graph_ = nullptr;
-    graph_k_ = 0;
+    for (auto& g : graphs_)
+        if (g) cudaGraphExecDestroy(g);
+    graphs_.clear();
 }
 
 template <class T>
@@ -159,8 +159,9 @@ void Engine::launch(int k, const Timer* timer) {
         ECK(cudaGetLastError());
         return;
     }
-    if (!graph_ || graph_k_ != k) {
-        drop_graph();
+    if ((int)graphs_.size() <= k) graphs_.resize(k + 1, nullptr);
+    cudaGraphExec_t& graph_ = graphs_[k];
+    if (!graph_) {
         cudaGraph_t g = nullptr;
         ECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < k; i++) launch_one_iteration(nullptr);
@@ -176,7 +177,6 @@ void Engine::launch(int k, const Timer* timer) {
             graph_ = nullptr;
             throw SolveError(std::string("CUDA graph instantiation failed: ") + cudaGetErrorString(e3), -6);
         }
-        graph_k_ = k;
     }
     ECK(cudaGraphLaunch(graph_, st_));
 }

@@ -50,7 +50,8 @@ public:
     // A member's descriptor changed (its Dev: the Green-operator table flag of a new process).
     void update_entry(int i, const BatchSolve& e);
     // Queue k iterations of every member that is iterating.  timer (may be null) wraps each
-    // launch, for per-kernel device times; without it the k iterations run as one CUDA graph.
+    // launch, for per-kernel device times; without it the k iterations run as one CUDA graph
+    // (one graph per k, captured at its first use).
     void launch(int k, const Timer* timer);
     // The members' event codes (EV_RUNNING, EV_CONVERGED, EV_ACCEPTED, EV_HOST or a status
     // code) after the queued work; synchronises the stream.
@@ -79,8 +80,7 @@ private:
     int* dEv_ = nullptr;
     int* hEv_ = nullptr;
     size_t capE_ = 0, capEv_ = 0;
-    cudaGraphExec_t graph_ = nullptr;
-    int graph_k_ = 0;
+    std::vector<cudaGraphExec_t> graphs_;  // graphs_[k]: k iterations captured (null until first used)
 };
 
 }  // namespace evp

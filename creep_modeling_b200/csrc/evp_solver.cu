@@ -88,6 +88,15 @@ struct Diag {
     double cond_sol = 0, cond_gas = 0, cond_cgas = 0;
     int imin_sol[3] = {0, 0, 0}, imin_gas[3] = {0, 0, 0};
 };
+// Iterations in one round: the expected count rounded down to a power of two and capped, so
+// that an engine holds at most four captured graphs (1, 2, 4 and 8 iterations).
+static constexpr int kMaxRound = 8;
+static int round_length(int want) {
+    int k = 1;
+    while (2 * k <= want && k < kMaxRound) k *= 2;
+    return k;
+}
+
 static double safe_rel(double x, double xp) { return (xp <= EVP_TINY || xp >= EVP_HUGE * 0.5) ? 0.0 : std::fabs(x - xp) / xp; }
 
 class Solver {
@@ -726,6 +735,7 @@ public:
         if (iter >= 100000) throw SolveError("equilibrium iteration did not converge", -4);
         if (restart) {  // roll the increment back and iterate it again with the cut time step
             iter = 0;
+            inc_launched = 0;
             snapshot(false);
             start_iterations();
             return false;
@@ -783,6 +793,7 @@ public:
         }
         K("k_prologue", [&] { launch_prologue(d, d_c0, d_g0, do_schmid, modal ? 1 : 0, st); });
         iter = 0;
+        inc_launched = 0;
         start_iterations();
         return true;
     }
@@ -799,6 +810,7 @@ public:
     void end_launch() {
         ProcessData& p = P();
         es.iter_done = iter;
+        prev_inc_iters = iter;
         if (p.iupdate == 1) {  // update_grid_velgrad_node reads L and F before update_defgrad changes F
             K("k_grid_fft", [&] {
                 launch_fft_x_fwd(d, pl1, 1, 0, st);
@@ -926,11 +938,23 @@ public:
         macrosteps_done++;
     }
 
+    // ------------------------------------------------------------ round length
+    // The host looks at the event codes after each round of queued iterations.  A solve expects
+    // its increment to take as many iterations as the previous one did, so a round ends where
+    // that expectation runs out instead of after a fixed count: a member that converges does not
+    // sit through the rest of a long round, and one far from convergence is not polled often.
+    int prev_inc_iters = 0;  // iterations of the previous increment (0: none yet)
+    int inc_launched = 0;    // iterations queued in this increment (since its last restart)
+    int want_iters() const {
+        if (prev_inc_iters <= 0) return 4;
+        const int rem = prev_inc_iters - inc_launched;
+        return rem > 0 ? rem : 2;  // past the expectation: look every two iterations
+    }
+
     // ------------------------------------------------------------ one macrostep of a solve on its own
-    // The engine of one member runs the increment's iterations; the host looks at the control
-    // block every check_every iterations (and at events: convergence, ITMAX, errors).
+    // The engine of one member runs the increment's iterations in rounds (round_length); the host
+    // looks at the control block between rounds (events: convergence, ITMAX, errors).
     std::unique_ptr<Engine> solo;
-    int check_every = 4;
     bool macrostep() {
         if (!begin_increment()) return false;
         if (!solo) {
@@ -941,12 +965,14 @@ public:
         }
         Engine::Timer timer = [this](const char* name, const std::function<void()>& f) { K(name, f); };
         const int per_iter = solo->launches_per_iteration();
-        long long rounds = 0;
+        long long queued = 0;
         while (true) {
             check_deadline();
-            if (++rounds > 100000 / check_every + 100) throw SolveError("equilibrium iteration did not converge", -4);
-            solo->launch(check_every, profile ? &timer : nullptr);
-            if (!profile) launches += (long long)check_every * per_iter;
+            const int k = round_length(want_iters());
+            if ((queued += k) > 100000 + 2 * kMaxRound) throw SolveError("equilibrium iteration did not converge", -4);
+            solo->launch(k, profile ? &timer : nullptr);
+            inc_launched += k;
+            if (!profile) launches += (long long)k * per_iter;
             const int ev = solo->read_events()[0];
             if (ev == EV_RUNNING) continue;
             pull_ctl();
@@ -1300,7 +1326,7 @@ public:
     std::vector<Slot> slots;  // slot ids stay valid; a removed slot keeps its record, not its solver
     std::vector<int> members;  // running slots, in the engine's member order
     bool dirty = false;
-    int check_every = 4;
+    int round_k = 0;  // iterations of the round in flight
 
     cudaEvent_t round_ev = nullptr;  // recorded after a launched round's iterations
     bool in_round = false;
@@ -1390,13 +1416,20 @@ public:
         dirty = false;
     }
 
-    // One round: check_every iterations of every running member (launch_round, asynchronous),
-    // then, once they have run (round_done), the host side of their events (finish_round).
+    // One round: a few iterations of every running member (launch_round, asynchronous), then,
+    // once they have run (round_done), the host side of their events (finish_round).  The round
+    // is as long as the member expected to stop first wants (round_length).
     bool launch_round() {
         if (in_round) return true;
         if (dirty) rebuild();
         if (members.empty()) return false;
-        eng->launch(check_every, nullptr);
+        int want = 1 << 30;
+        for (int id : members)
+            if (slots[id].s && slots[id].state == 0) want = std::min(want, slots[id].s->want_iters());
+        round_k = round_length(want);
+        eng->launch(round_k, nullptr);
+        for (int id : members)
+            if (slots[id].s && slots[id].state == 0) slots[id].s->inc_launched += round_k;
         CK(cudaEventRecord(round_ev, st));
         in_round = true;
         return true;
@@ -1415,7 +1448,7 @@ public:
             const int id = members[i];
             if (!slots[id].s || slots[id].state != 0) continue;
             Solver& s = *slots[id].s;
-            s.launches += (long long)check_every * per_iter;
+            s.launches += (long long)round_k * per_iter;
             try {
                 s.check_deadline();
                 if (ev[i] == EV_RUNNING) continue;
