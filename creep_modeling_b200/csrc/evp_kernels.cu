@@ -39,16 +39,36 @@ constexpr int kC0Block = 64;
 // partials[f * nblocks + block], in the body's block coordinates) -> the last block to finish folds them: one
 // warp per field, lane l adding blocks l, l + 32, ... in order, then a fixed
 // shuffle tree, so the result does not depend on timing.
+// The loads go out eight at a time (one L2 round trip per eight blocks instead of per block);
+// the additions keep the one-block-at-a-time order.
 __device__ __forceinline__ double fold_sum(const double* partials, int nblk, int f, int lane) {
+    const double* q = partials + (size_t)f * nblk;
     double s = 0.0;
-    for (int b = lane; b < nblk; b += 32) s += __ldcg(&partials[(size_t)f * nblk + b]);
+    int b = lane;
+    for (; b + 7 * 32 < nblk; b += 8 * 32) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = __ldcg(q + b + 32 * i);
+#pragma unroll
+        for (int i = 0; i < 8; i++) s += x[i];
+    }
+    for (; b < nblk; b += 32) s += __ldcg(q + b);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     return s;  // in lane 0
 }
 __device__ __forceinline__ double fold_max(const double* partials, int nblk, int f, int lane) {
+    const double* q = partials + (size_t)f * nblk;
     double s = -EVP_HUGE;
-    for (int b = lane; b < nblk; b += 32) s = fmax(s, __ldcg(&partials[(size_t)f * nblk + b]));
+    int b = lane;
+    for (; b + 7 * 32 < nblk; b += 8 * 32) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = __ldcg(q + b + 32 * i);
+#pragma unroll
+        for (int i = 0; i < 8; i++) s = fmax(s, x[i]);
+    }
+    for (; b < nblk; b += 32) s = fmax(s, __ldcg(q + b));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
     return s;  // in lane 0
@@ -1773,9 +1793,13 @@ static int newton_grid(const Dev& d, int variant) {
         const long long g = (d.N + kNewtonBlock - 1) / kNewtonBlock;
         return (int)(g < 148LL * 16 ? g : 148LL * 16);
     }
+    // one wave: the two blocks of 256 that fit each of the 148 SMs, every warp taking every
+    // (blocks x 8)-th batch of five voxels (measured on 64^3: 0.685 ms per launch against 0.766
+    // with 24 blocks per SM, where every block staged the phases, waited at its end for its
+    // slowest warp and folded its own sums)
     const long long warps = (d.N + 4) / 5;
     const long long g = (warps + 7) / 8;  // 8 warps per block of 256
-    return (int)(g < 148LL * 24 ? g : 148LL * 24);
+    return (int)(g < 148LL * 2 ? g : 148LL * 2);
 }
 static size_t newton_smem(const Dev& d, int variant) {
     switch (variant) {

@@ -182,6 +182,11 @@ public:
     // reducing the error: the FP32 round-off of the Green-operator update is about 1e-7 of the stress
     // heterogeneity, which can exceed the tolerance when the strain rates are very small (slow creep).
     int prec_it = 0;
+    // Mixed precision: an increment whose FP32 iterations stagnated (it finished in FP64) makes
+    // the next increments start in FP64; FP32 is tried again after 2, 4, ... 32 increments.
+    bool inc_fp32 = false;  // this increment started with FP32 spectra
+    int fp64_hold = 0;      // increments still to start in FP64
+    int fp64_len = 2;       // length of the next hold
     std::vector<double> err_hist;
     struct KTime {
         std::string name;
@@ -565,11 +570,12 @@ public:
         erre = 2.0 * p.error;
         errs = 2.0 * p.error;
         errsbc = 2.0 * p.error;
-        prec_it = prec;
+        inc_fp32 = prec != 0 && fp64_hold == 0;
+        prec_it = inc_fp32 ? 1 : 0;
         IterCtl& c = *h_ctl;
         std::memset(&c, 0, sizeof(c));
         c.active = 1;
-        c.prec = prec;
+        c.prec = prec_it;
         c.fresh = 1;
         c.sg_off = OFF_SGAVG;
         c.corr.mix = mix;
@@ -811,6 +817,16 @@ public:
         ProcessData& p = P();
         es.iter_done = iter;
         prev_inc_iters = iter;
+        if (prec) {
+            if (!inc_fp32) {
+                if (fp64_hold > 0) fp64_hold--;
+            } else if (prec_it == 0) {  // fell back to FP64
+                fp64_hold = fp64_len;
+                fp64_len = std::min(2 * fp64_len, 32);
+            } else {
+                fp64_len = 2;
+            }
+        }
         if (p.iupdate == 1) {  // update_grid_velgrad_node reads L and F before update_defgrad changes F
             K("k_grid_fft", [&] {
                 launch_fft_x_fwd(d, pl1, 1, 0, st);

@@ -111,3 +111,22 @@ def test_failing_member_leaves_the_others(tmp_path):
         assert all(b.status(s)["status"] == 0 for s in slots)
     for name, _, _ in members:
         _same(tmp_path / f"alone_{name}", tmp_path / f"batch_{name}")
+
+
+def test_members_sharing_one_newton_wave(tmp_path):
+    """Two 40^3 members, each with a full wave of local-solve blocks (296): the batched launch
+    runs two waves, and the members' files are identical to the solves alone."""
+    members = []
+    for i, stress in enumerate((120.0, 180.0)):
+        c = decks.case_c1(nsteps=3)
+        c.n, c.ngrains, c.seed = 40, 40, 11 + i
+        c.processes[0].stress33 = stress
+        members.append((f"c40_{i}", decks.write_case(c, tmp_path / f"c40_{i}"), 0))
+    for name, fft, prec in members:
+        _alone(fft, tmp_path / f"alone_{name}", prec)
+    with Batch() as b:
+        slots = [b.add(fft, tmp_path / f"batch_{name}") for name, fft, _ in members]
+        b.run()
+        assert all(b.status(s)["status"] == 0 for s in slots)
+    for name, _, _ in members:
+        _same(tmp_path / f"alone_{name}", tmp_path / f"batch_{name}")
