@@ -324,30 +324,33 @@ __device__ __forceinline__ void basis_T(const double* M, double* T) {
     }
 }
 // out = s * T A T^T (6x6)
+// (a row of T A at a time: six live values instead of 36, each sum in the same order)
 __device__ __forceinline__ void congruence6(const double* T, const double* A, double s, double* out) {
-    double TA[36];
 #pragma unroll
-    for (int i = 0; i < 6; i++)
+    for (int i = 0; i < 6; i++) {
+        double ta[6];
 #pragma unroll
         for (int j = 0; j < 6; j++) {
             double x = 0.0;
 #pragma unroll
             for (int k = 0; k < 6; k++) x += T[6 * i + k] * A[6 * k + j];
-            TA[6 * i + j] = x;
+            ta[j] = x;
         }
-#pragma unroll
-    for (int i = 0; i < 6; i++)
 #pragma unroll
         for (int j = 0; j < 6; j++) {
             double x = 0.0;
 #pragma unroll
-            for (int k = 0; k < 6; k++) x += TA[6 * i + k] * T[6 * j + k];
+            for (int k = 0; k < 6; k++) x += ta[k] * T[6 * j + k];
             out[6 * i + j] = s * x;
         }
+    }
 }
 
 // ---------------------------------------------------------------- k_prologue
-__global__ void __launch_bounds__(kBlock, 2) k_prologue(Dev d, const double* __restrict__ c0g, const double* __restrict__ g0g,
+// One block of 256 per SM at most (200 registers): the C~ congruence and its LU factors stay in
+// registers, where a two-block bound of 128 registers spilled ~0.5 kB per thread to local memory
+// (its write-back nearly doubled the kernel's DRAM writes).
+__global__ void __launch_bounds__(kBlock, 1) k_prologue(Dev d, const double* __restrict__ c0g, const double* __restrict__ g0g,
                                                        int do_schmid, int modal) {
     __shared__ double c0[81], g0[81], c0b[36];
     for (int i = threadIdx.x; i < 81; i += blockDim.x) {
@@ -369,12 +372,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_prologue(Dev d, const double* __r
             if (inv3u(aa, ai) != 0) set_err(d.err, 1);
             for (int s = 0; s < ph.nsyst; s++) {
                 double S[9], t[9], r[9], rs[9], b5[5];
+#pragma unroll
                 for (int i = 0; i < 3; i++)
+#pragma unroll
                     for (int j = 0; j < 3; j++) S[3 * i + j] = ph.dbca[3 * s + i] * ph.dnca[3 * s + j];
                 mm3(aa, S, t);
                 mm3(t, ai, r);
                 sym33(r, rs);
                 t2_to_b5(rs, b5);
+#pragma unroll
                 for (int c = 0; c < 5; c++) d.sch[(s * 5 + c) * N + v] = b5[c];
             }
         }
@@ -385,11 +391,19 @@ __global__ void __launch_bounds__(kBlock, 2) k_prologue(Dev d, const double* __r
         double c66[36], TF[36];
         basis_T(F, TF);
         congruence6(TF, c0b, 1.0 / detF, c66);
-        for (int c = 0; c < 36; c++) d.c066mod[c * N + v] = c66[c];
-        // its inverse, for the symmetric form of the local Newton system (in place: c066mod is stored)
-        if (inv_unrolled<6>(c66) != 0 && !gas) set_err(d.err, 1);
 #pragma unroll
-        for (int c = 0; c < 36; c++) d.c066inv[c * N + v] = c66[c];
+        for (int c = 0; c < 36; c++) d.c066mod[c * N + v] = c66[c];
+        // its inverse, for the symmetric form of the local Newton system, a column at a time from
+        // the LU factors (the bits of inv_unrolled without its identity block in registers)
+        int piv[6];
+        if (lu_unrolled<6>(c66, piv) != 0 && !gas) set_err(d.err, 1);
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            double x[6];
+            lu_inverse_column<6>(c66, piv, j, x);
+#pragma unroll
+            for (int i = 0; i < 6; i++) d.c066inv[(6 * i + j) * N + v] = x[i];
+        }
     }
 }
 // calc_c066mod_Goperr066mod, the modified augmented Lagrangian part (various_functions.f90:866-900):

@@ -335,6 +335,81 @@ EVP_HD int inv_unrolled(double* a) {
     for (int i = 0; i < n * n; i++) a[i] = B[i];
     return info;
 }
+// The factors of inv_unrolled's elimination, for inverting one column at a time (a third of
+// its registers: no identity block beside the matrix).  J ends with U in its upper triangle and,
+// below it, each step's multiplier numerators, moved with their rows by the later
+// interchanges; piv[k] is the row swapped with row k at step k.  Returns the dgetrf info value.
+template <int n>
+EVP_HD int lu_unrolled(double (&J)[n * n], int (&piv)[n]) {
+    int info = 0;
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double amax = fabs(J[k * n + k]);
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            double t = fabs(J[i * n + k]);
+            if (t > amax) { amax = t; p = i; }
+        }
+        piv[k] = p;
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int j = 0; j < n; j++) {
+                double x = J[k * n + j], y = J[i * n + j];
+                J[k * n + j] = sw ? y : x;
+                J[i * n + j] = sw ? x : y;
+            }
+        }
+        const double pv = J[k * n + k];
+        if (pv == 0.0 && info == 0) info = k + 1;
+        const double r = 1.0 / pv;
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const double l = J[i * n + k] * r;
+#pragma unroll
+            for (int j = k + 1; j < n; j++) J[i * n + j] -= l * J[k * n + j];
+        }
+    }
+    return info;
+}
+// Column j of the inverse from lu_unrolled's factors: the identity column through the same row
+// interchanges, the eliminations of inv_unrolled in the same order with the same multipliers
+// (each row takes its updates step by step either way), then its back substitution; the bits
+// equal column j of inv_unrolled's result.
+template <int n>
+EVP_HD void lu_inverse_column(const double (&J)[n * n], const int (&piv)[n], int j, double (&x)[n]) {
+    double b[n];
+#pragma unroll
+    for (int i = 0; i < n; i++) b[i] = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const bool sw = (piv[k] == i);
+            const double u = b[k], w = b[i];
+            b[k] = sw ? w : u;
+            b[i] = sw ? u : w;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+        const double r = 1.0 / J[k * n + k];
+#pragma unroll
+        for (int i = k + 1; i < n; i++) {
+            const double l = J[i * n + k] * r;
+            b[i] -= l * b[k];
+        }
+    }
+#pragma unroll
+    for (int i = n - 1; i >= 0; i--) {
+        double s = b[i];
+#pragma unroll
+        for (int m = i + 1; m < n; m++) s -= J[i * n + m] * x[m];
+        x[i] = s / J[i * n + i];
+    }
+}
 EVP_HD int inv3u(const double* a, double* ai) {
 #pragma unroll
     for (int i = 0; i < 9; i++) ai[i] = a[i];
