@@ -185,8 +185,9 @@ struct BatchSolve {
 struct Job {
     int solve, blk0, gx, gy, gz, tile;
 };
-// The passes of one equilibrium iteration, in launch order.
-enum BatchKind : int { BK_SGAVG, BK_XFWD, BK_YFWD, BK_ZGREEN, BK_YINV, BK_XINV, BK_CORR, BK_NEWTON, BK_N };
+// The passes of one equilibrium iteration, in launch order (the stress average that the first
+// iteration of an increment starts from is formed when the increment's iterations start).
+enum BatchKind : int { BK_XFWD, BK_YFWD, BK_ZGREEN, BK_YINV, BK_XINV, BK_CORR, BK_NEWTON, BK_N };
 struct BatchLaunch {
     int kind, variant;  // variant: FFT passes rs | (FP32 << 1); Newton: the kernel (newton_variant)
     int job0, njobs;    // slice of the plan's job table

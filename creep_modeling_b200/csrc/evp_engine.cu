@@ -36,8 +36,8 @@ cudaMemPool_t solver_pool() {
 }
 
 static const char* kind_name(int k) {
-    static const char* names[BK_N] = {"k_sgavg", "k_fft_x_fwd", "k_fft_y_fwd", "k_fft_z_green",
-                                      "k_fft_y_inv", "k_fft_x_inv", "k_corr", "k_newton"};
+    static const char* names[BK_N] = {"k_fft_x_fwd", "k_fft_y_fwd", "k_fft_z_green", "k_fft_y_inv",
+                                      "k_fft_x_inv", "k_corr", "k_newton"};
     return (k >= 0 && k < BK_N) ? names[k] : "k_batched";
 }
 static bool fft_kind(int k) { return k == BK_XFWD || k == BK_YFWD || k == BK_ZGREEN || k == BK_YINV || k == BK_XINV; }

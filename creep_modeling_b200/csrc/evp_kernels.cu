@@ -1865,12 +1865,6 @@ void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
 // the member's control block and runs the same body as the member's single-solve
 // launch, on the member's own block coordinates.  Blocks of members that are not
 // iterating (converged, waiting for the host) exit at once.
-__global__ void __launch_bounds__(kBlock) kb_sgavg(const __grid_constant__ BatchParams P) {
-    const Job& jb = batch_job(P);
-    const BatchSolve& m = P.E[jb.solve];
-    if (!(m.ctl->active && m.ctl->fresh)) return;  // uniform over the block
-    body_sgavg(m.d, job_vb(jb));
-}
 __global__ void __launch_bounds__(kBlock, 2) kb_corr(const __grid_constant__ BatchParams P) {
     __shared__ CorrParams p;
     __shared__ int go;
@@ -1916,7 +1910,6 @@ void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj) {
         mj.smem[0][k] = sm;
         mj.variant[0][k] = variant;
     };
-    one_d(BK_SGAVG, d.grid, kBlock, 0, 0);
     one_d(BK_CORR, d.grid < 148 * 2 ? d.grid : 148 * 2, kBlock, 0, 0);
     const int v = newton_variant(d, modal);
     one_d(BK_NEWTON, newton_grid(d, v), v >= 6 ? kNewtonBlock : 256, newton_smem(d, v), v);
@@ -1924,7 +1917,6 @@ void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj) {
 
 void launch_batched_voxel(const BatchLaunch& L, const BatchParams& P, cudaStream_t st) {
     switch (L.kind) {
-        case BK_SGAVG: kb_sgavg<<<L.blocks, L.threads, 0, st>>>(P); break;
         case BK_CORR: kb_corr<<<L.blocks, L.threads, 0, st>>>(P); break;
         case BK_NEWTON:
             switch (L.variant) {

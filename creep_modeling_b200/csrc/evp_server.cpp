@@ -10,7 +10,8 @@
 // running batch as soon as memory and a slot free up, and their work shares the
 // launches of every solve already on the device.  Finished solves (their files
 // written) leave the batch at once.  Two batches run side by side: small grids on a
-// stream of the highest priority, the others on the lowest, each with its own rounds.
+// stream of the highest priority, the others on the lowest, each with its own rounds;
+// the second holds a bounded number of voxels, so the shortest large requests run first.
 #include "../../include/evp.h"
 #include "evp_batch.h"
 #include "evp_deck.h"
@@ -73,6 +74,12 @@ double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::dura
 // device's highest priority, so their short rounds get SMs ahead of the large lane's long ones
 // and a small request's latency does not follow the round time of the largest solves.
 constexpr long long kSmallLaneVoxels = 40LL * 40 * 40;
+// The large lane holds at most this many voxels at once (two 64^3 solves; a larger solve runs
+// alone there).  One such solve already fills every launch of an iteration, so admitting more
+// would only share the GPU among them (each finishing late) where admitting the least work first
+// and few at a time lets the short requests finish early, at the same throughput.
+constexpr long long kLargeLaneVoxels = 2LL * 64 * 64 * 64;
+static int lane_of(long long voxels) { return voxels <= kSmallLaneVoxels ? 0 : 1; }
 
 struct evp_server {
     std::mutex m;
@@ -83,6 +90,7 @@ struct evp_server {
     std::thread engine;
     unsigned long long budget = 0, used = 0, next_id = 1;
     int max_inflight = 16, inflight = 0, device = 0;
+    long long lane_vox[2] = {0, 0};  // voxels of the solves running in each lane
     bool closing = false;
     std::string fatal;  // a CUDA failure of the engine: every later request fails with it
 
@@ -103,6 +111,8 @@ struct evp_server {
         for (auto id : queue) {
             const Request& r = reqs[id];
             if (used + r.foot > budget && inflight > 0) continue;  // a request larger than the budget runs alone
+            const long long vox = (long long)r.n1 * r.n2 * r.n3;
+            if (lane_of(vox) == 1 && lane_vox[1] > 0 && lane_vox[1] + vox > kLargeLaneVoxels) continue;
             if (best == 0 || r.work < best_work) {
                 best = id;
                 best_work = r.work;
@@ -146,7 +156,9 @@ struct evp_server {
                 const std::string fft = r.fft, out = r.out;
                 const int mix = r.mix, modal = r.modal, flags = r.flags;
                 const double dl = r.deadline_s;
-                const int l = (long long)r.n1 * r.n2 * r.n3 <= kSmallLaneVoxels ? 0 : 1;
+                const long long vox = (long long)r.n1 * r.n2 * r.n3;
+                const int l = lane_of(vox);
+                lane_vox[l] += vox;
                 lk.unlock();
                 std::string err;
                 int slot = -1;
@@ -165,6 +177,7 @@ struct evp_server {
                     complete(q, status, err, rep.macrosteps, rep.voxel_iters);
                     if (slot >= 0) evp::batch_remove(lane[l].get(), slot);
                     used -= q.foot;
+                    lane_vox[l] -= vox;
                     inflight--;
                     cv.notify_all();
                 } else {
@@ -220,6 +233,7 @@ struct evp_server {
                     complete(q, status, err, rep.macrosteps, rep.voxel_iters);
                     if (st == 1 || !pending[it->first.first]) evp::batch_remove(b, it->first.second);
                     used -= q.foot;
+                    lane_vox[it->first.first] -= (long long)q.n1 * q.n2 * q.n3;
                     inflight--;
                     it = slot_req.erase(it);
                 } else {

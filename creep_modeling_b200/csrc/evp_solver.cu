@@ -635,6 +635,9 @@ public:
         c.tdot = p.tdot;
         c.tdotref = p.tdotref;
         h2d_copy(d_ctl, h_ctl, sizeof(IterCtl));
+        // the weighted stress average the first iteration starts from (LS-EVPFFT.f90:238-252; later
+        // iterations take it from the previous Newton launch's sums of the same stresses)
+        K("k_sgavg", [&] { launch_sgavg(d, st); });
     }
 
     // The control block back on the host once the device has stopped the iteration (an event).

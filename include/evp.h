@@ -177,6 +177,9 @@ int evp_solve_files(int n, const char* const* fft_in, const char* const* out_dir
  * (continuous batching), and a solve that finishes leaves it at once.  Solves of
  * at most 40^3 voxels run in a second batch on a stream of the highest priority,
  * with rounds of their own, so small requests are not paced by the largest ones.
+ * The batch of larger solves holds at most 2 x 64^3 voxels at once (a larger
+ * solve runs alone in it): one such solve already fills the GPU, so the queue's
+ * shortest requests finish first instead of all of them sharing the device.
  * A solve's results do not depend on what else runs beside it. */
 typedef struct evp_server evp_server;
 
