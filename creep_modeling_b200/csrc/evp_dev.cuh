@@ -232,6 +232,26 @@ __device__ __forceinline__ VB job_vb(const Job& jb) {
     const int l = (int)blockIdx.x - jb.blk0;
     return VB{l % jb.gx, (l / jb.gx) % jb.gy, l / (jb.gx * jb.gy), jb.gx};
 }
+// Sum of field f of nblk block partials (partials[f * nblk + b]) by one warp: lane l adds
+// blocks l, l + 32, ... in order, then a fixed shuffle tree; the result is in lane 0.
+// The loads go out eight at a time (one L2 round trip per eight blocks instead of per block);
+// the additions keep the one-block-at-a-time order.
+__device__ __forceinline__ double fold_sum(const double* partials, int nblk, int f, int lane) {
+    const double* q = partials + (size_t)f * nblk;
+    double s = 0.0;
+    int b = lane;
+    for (; b + 7 * 32 < nblk; b += 8 * 32) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = __ldcg(q + b + 32 * i);
+#pragma unroll
+        for (int i = 0; i < 8; i++) s += x[i];
+    }
+    for (; b < nblk; b += 32) s += __ldcg(q + b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    return s;  // in lane 0
+}
 #endif
 
 // ---- launch wrappers (stream-ordered)

@@ -722,9 +722,7 @@ __device__ __forceinline__ void body_fft_x_inv(const Dev& d, const FftPlan1D& pl
     if (last) {  // fold the block partials: one warp per field, fixed order
         __threadfence();
         for (int f = warp; f < 9; f += nw) {
-            double x = 0.0;
-            for (int b = lane; b < vb.nx; b += 32) x += __ldcg(&d.partials[(size_t)f * vb.nx + b]);
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            const double x = fold_sum(d.partials, vb.nx, f, lane);
             if (lane == 0) fsum[f] = x;
         }
         __syncthreads();

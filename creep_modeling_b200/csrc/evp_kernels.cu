@@ -38,25 +38,8 @@ constexpr int kC0Block = 64;
 // NS sums then NM maxima per thread -> one partial per block (stored field-major,
 // partials[f * nblocks + block], in the body's block coordinates) -> the last block to finish folds them: one
 // warp per field, lane l adding blocks l, l + 32, ... in order, then a fixed
-// shuffle tree, so the result does not depend on timing.
-// The loads go out eight at a time (one L2 round trip per eight blocks instead of per block);
-// the additions keep the one-block-at-a-time order.
-__device__ __forceinline__ double fold_sum(const double* partials, int nblk, int f, int lane) {
-    const double* q = partials + (size_t)f * nblk;
-    double s = 0.0;
-    int b = lane;
-    for (; b + 7 * 32 < nblk; b += 8 * 32) {
-        double x[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) x[i] = __ldcg(q + b + 32 * i);
-#pragma unroll
-        for (int i = 0; i < 8; i++) s += x[i];
-    }
-    for (; b < nblk; b += 32) s += __ldcg(q + b);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    return s;  // in lane 0
-}
+// shuffle tree, so the result does not depend on timing (fold_sum, in evp_dev.cuh, for the
+// sums; fold_max for the maxima).
 __device__ __forceinline__ double fold_max(const double* partials, int nblk, int f, int lane) {
     const double* q = partials + (size_t)f * nblk;
     double s = -EVP_HUGE;
@@ -2313,7 +2296,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_diag(Dev d, double Lfloor) {
     if (lastblk && threadIdx.x == 0) {
         __threadfence();
         MinIdx a = {EVP_HUGE, -1}, b = {EVP_HUGE, -1};
-        for (unsigned q = 0; q < gridDim.x; q++) {
+        unsigned q = 0;
+        for (; q + 8 <= gridDim.x; q += 8) {  // eight blocks' pairs loaded at a time, folded in block order
+            MinIdx x[8], y[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                x[i] = MinIdx{__ldcg(&pm[2 * (q + i)].v), __ldcg(&pm[2 * (q + i)].i)};
+                y[i] = MinIdx{__ldcg(&pm[2 * (q + i) + 1].v), __ldcg(&pm[2 * (q + i) + 1].i)};
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                a = min_last(a, x[i]);
+                b = min_last(b, y[i]);
+            }
+        }
+        for (; q < gridDim.x; q++) {
             MinIdx x = {__ldcg(&pm[2 * q].v), __ldcg(&pm[2 * q].i)};
             MinIdx y = {__ldcg(&pm[2 * q + 1].v), __ldcg(&pm[2 * q + 1].i)};
             a = min_last(a, x);

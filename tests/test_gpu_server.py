@@ -112,3 +112,32 @@ def test_failing_solves_are_isolated(tmp_path):
     assert s_slow["run_s"] < 30.0
     for i in range(len(good)):
         _same(tmp_path / f"alone{i}", tmp_path / f"mix{i}")
+
+
+def test_large_lane_runs_the_shortest_first(tmp_path):
+    """Three 72^3 requests (373,248 voxels each; the large lane holds at most 2 x 64^3 =
+    524,288 voxels, so one at a time there) submitted back to back: their runs do not overlap,
+    and the two that queue behind the first (a longer one, so that both are queued when it ends)
+    are admitted least work first (voxels x increments)."""
+    import time
+
+    nsteps = (20, 4, 2)
+    ffts = []
+    for i, k in enumerate(nsteps):
+        c = decks.case_c1(nsteps=k)
+        c.n, c.ngrains = 72, 40
+        ffts.append(decks.write_case(c, tmp_path / f"d{i}"))
+    with Server(0, 8) as srv:
+        t0 = time.perf_counter()
+        calls, tickets = [], []
+        for i, f in enumerate(ffts):  # each submit reads its deck (~0.1 s at 72^3) on this thread
+            calls.append(time.perf_counter() - t0)
+            tickets.append(srv.submit(f, tmp_path / f"o{i}", mix=1, modal=0, csv_only=True))
+        sts = [srv.wait(t, timeout=600) for t in tickets]
+    assert all(st["status"] == 0 for st in sts), sts
+    start = [calls[i] + sts[i]["queued_s"] for i in range(3)]
+    end = [start[i] + sts[i]["run_s"] for i in range(3)]
+    order = sorted(range(3), key=lambda i: start[i])
+    for p, q in zip(order, order[1:]):
+        assert start[q] >= end[p] - 0.01, (start, end, sts)
+    assert order == [0, 2, 1], (order, start, end)
