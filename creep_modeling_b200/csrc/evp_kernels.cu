@@ -2039,14 +2039,18 @@ __global__ void __launch_bounds__(kBlock) k_upd2(Dev d, Upd2Params p) {
             st9(d.Fe, N, v, Fe);
             st9(d.Feinc, N, v, Feinc);
             // update_el_stiff (various_functions.f90:2327-2402)
-            double ag[9], aa[9], c4[81], c66[36];
+            // (the rotation of the crystal stiffness by aa = Fe ag as two 6x6 products in the
+            // b-basis, Q c Q^T with Q = rot_b66(aa), instead of index by index over 3x3x3x3 and
+            // chg_basis: the same tensor, rounding apart)
+            double ag[9], aa[9], Q[36], cc[36], c66[36];
             ld9(d.ag, N, v, ag);
             mm3(Fe, ag, aa);
             const double detFe = det33(Fe);
-            rotate4(aa, ph.C, c4);
-            for (int c = 0; c < 81; c++) c4[c] = c4[c] / detFe;
-            t4_to_b66(c4, c66);
+            rot_b66(aa, Q);
+            t4_to_b66(ph.C, cc);
+            congruence6(Q, cc, 1.0 / detFe, c66);
             if (inv_unrolled<6>(c66) != 0) set_err(d.err, 1);
+#pragma unroll
             for (int c = 0; c < 36; c++) d.sg66[c * N + v] = c66[c];
         } else {
             ld9(d.Feinc, N, v, Feinc);
@@ -2368,8 +2372,11 @@ __global__ void __launch_bounds__(kC0Block) k_c0(Dev d, double tdot, double tdot
 }
 void launch_c0(const Dev& d, double tdot, double tdotref, cudaStream_t st) {
     const size_t sm = (size_t)kC0Block * 72 * sizeof(double);
+    // four blocks per SM (the 255-register bound allows four of 64 threads): one wave, each
+    // thread several voxels, and a fold of 592 block partials per field instead of 2368
+    // (measured 624 -> 498 us at 64^3)
     const long long g = (d.N + kC0Block - 1) / kC0Block;
-    const int grid = (int)(g < 148LL * 16 ? g : 148LL * 16);
+    const int grid = (int)(g < 148LL * 4 ? g : 148LL * 4);
     if (d.nsys <= 12) {
         cudaFuncSetAttribute(k_c0<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_c0<12><<<grid, kC0Block, sm, st>>>(d, tdot, tdotref);

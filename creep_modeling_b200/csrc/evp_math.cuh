@@ -704,6 +704,49 @@ EVP_HD void rotate4(const double* A, const double* in, double* out) {
         double s = 0; for (int L = 0; L < 3; L++) s += A[3 * l + L] * t1[ijk * 3 + L]; out[ijk * 3 + l] = s; }
 }
 
+// The b-basis form of the rotation c'_ijkl = a_ip a_jq a_kr a_ls c_pqrs of a fourth-order tensor
+// with minor symmetries: c'66 = Q c66 Q^T with Q_ag = <B^a, a B^g a^T> (Frobenius product; B^0..B^5
+// the symmetric basis of chg_basis, complete for symmetric 3x3 tensors).  Q[6 * a + g].
+EVP_HD void rot_b66(const double* a, double* Q) {
+#pragma unroll
+    for (int g = 0; g < 6; g++) {
+        const BasisNZ bg = basis_nz(g);
+        double Bg[9], t[9], M[9];
+#pragma unroll
+        for (int c = 0; c < 9; c++) Bg[c] = 0.0;
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+            if (p < bg.n) Bg[bg.idx[p]] = bg.v[p];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                double s = 0.0;
+#pragma unroll
+                for (int k = 0; k < 3; k++) s += a[3 * i + k] * Bg[3 * k + j];
+                t[3 * i + j] = s;
+            }
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                double s = 0.0;
+#pragma unroll
+                for (int k = 0; k < 3; k++) s += t[3 * i + k] * a[3 * j + k];
+                M[3 * i + j] = s;
+            }
+#pragma unroll
+        for (int al = 0; al < 6; al++) {
+            const BasisNZ ba = basis_nz(al);
+            double s = 0.0;
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+                if (p < ba.n) s += ba.v[p] * M[ba.idx[p]];
+            Q[6 * al + g] = s;
+        }
+    }
+}
+
 // euler(iopt=2) (tensor_functions.f90:550-566)
 EVP_HD void euler2(double ph, double th, double tm, double* a) {
     double sph = sin(ph), cph = cos(ph), sth = sin(th), cth = cos(th), stm = sin(tm), ctm = cos(tm);
