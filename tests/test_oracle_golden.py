@@ -1,6 +1,6 @@
 """Pins the CPU oracle's building blocks against numpy/scipy golden vectors and analytic known answers.
 
-The reference ships no golden vectors; these fixtures are
+The reference ships no golden vectors (it has no tests); these fixtures are
 generated by tests/golden/make_golden.py from independent implementations.
 """
 from pathlib import Path
