@@ -99,3 +99,15 @@ def test_power_law_single_slip(orc):
         assert abs(gd[0] - expect) <= 1e-14 * abs(expect)
         assert abs(e6[4] - expect) <= 1e-14 * abs(expect)
         assert abs(d.reshape(6, 6)[4, 4] - n * 1e-3 * abs(sig5 / tauc) ** (n - 1) / tauc) <= 1e-13 * abs(d[28])
+
+
+def test_single_crystal_elastic_known_answer(orc, tmp_path):
+    """The oracle's whole solve on a homogeneous elastic single crystal reproduces the cubic
+    compliance (tests/single_crystal.py)."""
+    from tests import single_crystal as sc
+
+    fft = sc.write_deck(tmp_path / "deck")
+    o = orc.OracleSolve(str(fft), out_dir=str(tmp_path / "out"), mix=1, modal=0, write_files=True)
+    o.run()
+    o.close()
+    sc.check_first_increment(tmp_path / "out" / "results.csv")
