@@ -67,6 +67,9 @@ def lib():
         L.oracle_plastic_rate.argtypes = [c_dp, c_dp, c_dp, c_dp, ctypes.c_int, c_dp, c_dp, c_dp, c_dp]
         L.oracle_green_apply.argtypes = [c_dp, c_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp]
         L.oracle_green_apply.restype = ctypes.c_int
+        L.oracle_harden.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, c_dp, c_dp,
+                                    ctypes.c_double, c_dp, ctypes.c_double, c_dp]
+        L.oracle_harden.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -183,6 +186,19 @@ def polar(f):
 def cond1(a66):
     a = np.ascontiguousarray(a66, dtype=np.float64).reshape(36)
     return float(lib().oracle_cond1_6x6(_p(a)))
+
+
+def harden(tau1, thet0, thet1, hard, gamdot, gamma0, crss, tdot):
+    """The oracle's harden (various_functions.f90:1439-1491) for one voxel of a one-mode phase:
+    new resistances [nsyst, 2] and the new accumulated shear."""
+    hard = np.ascontiguousarray(hard, dtype=np.float64)
+    gamdot = np.ascontiguousarray(gamdot, dtype=np.float64)
+    crss = np.ascontiguousarray(crss, dtype=np.float64)
+    n = gamdot.size
+    out = np.zeros((n, 2))
+    g1 = lib().oracle_harden(n, float(tau1), float(thet0), float(thet1), _p(hard), _p(gamdot), float(gamma0), _p(crss),
+                             float(tdot), _p(out))
+    return out, g1
 
 
 def green_apply(tau: np.ndarray, shape, c0: np.ndarray, s0: np.ndarray) -> np.ndarray:

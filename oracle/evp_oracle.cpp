@@ -937,11 +937,13 @@ struct Oracle {
 
     // ------------------------------------------------------------ harden (various_functions.f90:1439-1491)
     void harden(const Voxel& x, double tau[NSYSMX][2], double& gamma1) const {
-        const Phase& ph = phase[x.phase - 1];
-        double tdot = process[ipr - 1].tdot;
+        harden_rates(phase[x.phase - 1], x.gamdot, x.gacumgr, x.crss, process[ipr - 1].tdot, tau, gamma1);
+    }
+    // the same on explicit arguments: slip rates, accumulated shear and committed resistances
+    static void harden_rates(const Phase& ph, const double* gamdot, double gamma0, const double (*crss)[2], double tdot,
+                             double tau[NSYSMX][2], double& gamma1) {
         double deltgam = 0.0;
-        for (int is = 0; is < ph.nsyst; is++) deltgam = deltgam + std::fabs(x.gamdot[is]) * tdot;
-        double gamma0 = x.gacumgr;
+        for (int is = 0; is < ph.nsyst; is++) deltgam = deltgam + std::fabs(gamdot[is]) * tdot;
         gamma1 = gamma0 + deltgam;
         int is = 0, islast = 0;
         std::memset(tau, 0, sizeof(double) * NSYSMX * 2);
@@ -953,9 +955,9 @@ struct Oracle {
             double voce = deltgam * thet1 + tau1 * (exp0 - exp1) + thet1 * (gamma0 * exp0 - gamma1 * exp1);
             for (int ism = 0; ism < ph.nsm[mode]; ism++) {
                 double dtau = 0.;
-                for (int js = 0; js < ph.nsyst; js++) dtau = dtau + ph.hard[is][js] * std::fabs(x.gamdot[js]);
-                tau[is][0] = x.crss[is][0] + dtau * voce * tdot / deltgam;
-                tau[is][1] = x.crss[is][1] + dtau * voce * tdot / deltgam;
+                for (int js = 0; js < ph.nsyst; js++) dtau = dtau + ph.hard[is][js] * std::fabs(gamdot[js]);
+                tau[is][0] = crss[is][0] + dtau * voce * tdot / deltgam;
+                tau[is][1] = crss[is][1] + dtau * voce * tdot / deltgam;
                 is++;
             }
         }
@@ -2199,6 +2201,35 @@ int oracle_green_apply(const double* tau9, double* out9, int n1, int n2, int n3,
         return -1;
     }
     return 0;
+}
+
+// harden for one voxel of a one-mode phase: nsyst systems with Voce parameters tau1, thet0, thet1,
+// the latent-hardening matrix hard (nsyst x nsyst, row-major), slip rates gamdot, accumulated shear
+// gamma0 and committed resistances crss (nsyst x 2) over a step tdot; new resistances in tau_out.
+double oracle_harden(int nsyst, double tau1, double thet0, double thet1, const double* hard, const double* gamdot,
+                     double gamma0, const double* crss_nx2, double tdot, double* tau_out) {
+    Phase ph;
+    ph.nsyst = nsyst;
+    ph.nmodes = 1;
+    ph.nsm[0] = nsyst;
+    for (int s = 0; s < nsyst; s++) {
+        ph.tau[s][2] = tau1;
+        ph.thet[s][0] = thet0;
+        ph.thet[s][1] = thet1;
+        for (int t = 0; t < nsyst; t++) ph.hard[s][t] = hard[nsyst * s + t];
+    }
+    double cr[NSYSMX][2], tau[NSYSMX][2], gamma1 = 0.0, gd[NSYSMX] = {};
+    for (int s = 0; s < nsyst; s++) {
+        cr[s][0] = crss_nx2[2 * s];
+        cr[s][1] = crss_nx2[2 * s + 1];
+        gd[s] = gamdot[s];
+    }
+    Oracle::harden_rates(ph, gd, gamma0, cr, tdot, tau, gamma1);
+    for (int s = 0; s < nsyst; s++) {
+        tau_out[2 * s] = tau[s][0];
+        tau_out[2 * s + 1] = tau[s][1];
+    }
+    return gamma1;
 }
 
 void oracle_plastic_rate(const double* sch5xn, const double* trialtau_nx2, const double* nrs, const double* gamd0, int nsyst,

@@ -69,6 +69,11 @@ void oracle_plastic_rate(const double* sch5xn, const double* trialtau_nx2,
                          const double* nrs, const double* gamd0, int nsyst,
                          const double* sg6, double* edotp6, double* dedotp66,
                          double* gamdot);
+/* harden (various_functions.f90:1439-1491) for one voxel of a one-mode phase: new resistances
+ * (nsyst x 2) in tau_out; returns the new accumulated shear. */
+double oracle_harden(int nsyst, double tau1, double thet0, double thet1, const double* hard,
+                     const double* gamdot, double gamma0, const double* crss_nx2, double tdot,
+                     double* tau_out);
 
 #ifdef __cplusplus
 }

@@ -111,3 +111,21 @@ def test_single_crystal_elastic_known_answer(orc, tmp_path):
     o.run()
     o.close()
     sc.check_first_increment(tmp_path / "out" / "results.csv")
+
+
+def test_harden_is_the_exact_voce_increment(orc):
+    """With a latent-hardening matrix of ones, harden's resistance increment is the Voce law's own
+    increment tau(G1) - tau(G0), tau(G) = (tau1 + thet1 G)(1 - exp(-thet0 G / tau1)), G the
+    accumulated shear (the reference integrates the law exactly over the step)."""
+    rng = np.random.default_rng(5)
+    tau1, thet0, thet1 = 40.0, 500.0, 20.0
+    n = 12
+    voce = lambda g: (tau1 + thet1 * g) * (1.0 - np.exp(-thet0 * g / tau1))
+    for gamma0, tdot in ((0.0, 10.0), (0.013, 0.5), (0.2, 2.0)):
+        gamdot = rng.uniform(-1e-4, 1e-4, n)
+        crss = rng.uniform(90.0, 110.0, (n, 2))
+        tau, g1 = orc.harden(tau1, thet0, thet1, np.ones((n, n)), gamdot, gamma0, crss, tdot)
+        dg = np.sum(np.abs(gamdot)) * tdot
+        assert abs(g1 - (gamma0 + dg)) <= 1e-15 * (gamma0 + dg)
+        inc = voce(gamma0 + dg) - voce(gamma0)
+        assert np.allclose(tau - crss, inc, rtol=1e-10, atol=1e-12 * tau1), (tau - crss, inc)
