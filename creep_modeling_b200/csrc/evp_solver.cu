@@ -19,6 +19,7 @@
 #include <chrono>
 #include <filesystem>
 #include <functional>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -158,6 +159,12 @@ public:
         return (T*)p;
     }
     ~Solver() {
+        if (vtk_job.valid()) {
+            try {
+                vtk_job.get();
+            } catch (...) {
+            }
+        }
         solo.reset();
         for (void* p : allocs) cudaFreeAsync(p, st);
         if (st) cudaStreamSynchronize(st);
@@ -177,6 +184,14 @@ public:
     // ---- host<->device byte counters and the optional per-kernel event timer
     long long h2d = 0, d2h = 0;
     bool profile = false, write_vtk_files = false;
+    // VTK files are formatted and written by a background task (one at a time) while the solve
+    // goes on, when the caller only needs the files at the end of the solve (evp_solve_file, a
+    // batch or server member); wait_vtk() finishes the last one and reports its error.
+    bool async_vtk = false;
+    std::future<void> vtk_job;
+    void wait_vtk() {
+        if (vtk_job.valid()) vtk_job.get();
+    }
     int prec = 0;  // 1: mixed precision (FP32 spectrum, FFTs and Green operator in the equilibrium chain)
     // Mixed precision falls back to FP64 for the rest of an increment once its FP32 iterations stop
     // reducing the error: the FP32 round-off of the Green-operator update is about 1e-7 of the stress
@@ -1145,21 +1160,38 @@ public:
         }
     }
 
-    void write_vtk(int istp) {  // write_vtk_cell (IO_functions.f90:945-1235)
+    // write_vtk_cell (IO_functions.f90:945-1235): the fields are copied to the host here, in the
+    // solve's stream order; the text is formatted and written by vtk_file, in the background when
+    // async_vtk is set.
+    void write_vtk(int istp) {
+        wait_vtk();
         const long long N = d.N;
         const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
-        auto xn = field_host(d.xnode, 3 * (size_t)(n1 + 1) * (n2 + 1) * d.n3node);
-        auto gd = field_host(d.gamdot, (size_t)d.nsys * N);
-        auto ga = field_host(d.gacumgr, N);
-        auto fp = field_host(d.Fp, 9 * N);
-        auto sg = field_host(d.sg, 6 * N);
-        auto F = field_host(d.F, 9 * N);
-        auto dF = field_host(d.detF, N);
-        auto ep = field_host(d.epvm, N);
-        auto vg = field_host(d.velgrad, 9 * N);
+        VtkFields v;
+        v.xn = field_host(d.xnode, 3 * (size_t)(n1 + 1) * (n2 + 1) * d.n3node);
+        v.gd = field_host(d.gamdot, (size_t)d.nsys * N);
+        v.ga = field_host(d.gacumgr, N);
+        v.fp = field_host(d.Fp, 9 * N);
+        v.sg = field_host(d.sg, 6 * N);
+        v.F = field_host(d.F, 9 * N);
+        v.dF = field_host(d.detF, N);
+        v.ep = field_host(d.epvm, N);
+        v.vg = field_host(d.velgrad, 9 * N);
         char name[64];
         std::snprintf(name, sizeof(name), "microstr_cell_fields_stp_%05d.vtk", istp);
-        std::string path = outdir + "/" + name;
+        auto job = [this, path = outdir + "/" + name, v = std::move(v)]() { vtk_file(path, v); };
+        if (async_vtk) vtk_job = std::async(std::launch::async, std::move(job));
+        else job();
+    }
+    struct VtkFields {
+        std::vector<double> xn, gd, ga, fp, sg, F, dF, ep, vg;
+    };
+    // the file itself, from host copies and the deck's grain and phase ids (read-only here)
+    void vtk_file(const std::string& path, const VtkFields& v) const {
+        const long long N = d.N;
+        const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+        const std::vector<double>&xn = v.xn, &gd = v.gd, &ga = v.ga, &fp = v.fp, &sg = v.sg, &F = v.F, &dF = v.dF,
+                                   &ep = v.ep, &vg = v.vg;
         FILE* f = std::fopen(path.c_str(), "w");
         if (!f) throw SolveError("ioerr in writevtk", -5);
         char b[256];
@@ -1369,9 +1401,25 @@ public:
     void finish(int id, int status, const std::string& err) {
         Slot& sl = slots[id];
         if (sl.state == 1) return;
+        std::string e = err;
+        if (sl.s) {  // the member's last VTK file is complete before it is reported done
+            try {
+                sl.s->wait_vtk();
+            } catch (SolveError& x) {
+                if (status == 0) {
+                    status = x.code;
+                    e = x.what();
+                }
+            } catch (std::exception& x) {
+                if (status == 0) {
+                    status = -1;
+                    e = x.what();
+                }
+            }
+        }
         sl.state = 1;
         sl.status = status;
-        sl.err = err;
+        sl.err = e;
         std::memset(&sl.rep, 0, sizeof(sl.rep));
         if (sl.s) {
             Solver& s = *sl.s;
@@ -1396,6 +1444,7 @@ public:
         slots[id].t0 = std::chrono::steady_clock::now();
         slots[id].s.reset(new Solver());
         Solver& s = *slots[id].s;
+        s.async_vtk = true;  // a member's files are needed when it finishes (finish waits for them)
         try {
             s.open(fft_in, out, mix, modal, flags & ~EVP_PROFILE, st, &dk);
             if (deadline_s > 0.0) {
@@ -1580,10 +1629,13 @@ int evp_version(void) { return 1; }
 
 const char* evp_last_error(void) { return evp::g_last_error.c_str(); }
 
-int evp_open(const char* fft_in, const char* out_dir, int mix, int modal, int flags, evp_solve** out) {
+// async_vtk: VTK files (the step-0 one included) written in the background, finished by wait_vtk
+static int open_solve(const char* fft_in, const char* out_dir, int mix, int modal, int flags, bool async_vtk,
+                      evp_solve** out) {
     if (!fft_in || !out) return fail("evp_open: null argument", -7);
     *out = nullptr;
     evp_solve* h = new evp_solve();
+    h->s.async_vtk = async_vtk;
     try {
         h->s.open(fft_in, out_dir ? out_dir : "", mix, modal, flags);
     } catch (SolveError& e) {
@@ -1595,6 +1647,10 @@ int evp_open(const char* fft_in, const char* out_dir, int mix, int modal, int fl
     }
     *out = h;
     return 0;
+}
+
+int evp_open(const char* fft_in, const char* out_dir, int mix, int modal, int flags, evp_solve** out) {
+    return open_solve(fft_in, out_dir, mix, modal, flags, false, out);
 }
 
 int evp_advance(evp_solve* h, int nmacro, int* done) {
@@ -1825,7 +1881,8 @@ int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const 
     if (fftw_save && fftw_save[0]) evp_tune_cache(fftw_save);
     auto t0 = std::chrono::steady_clock::now();
     evp_solve* h = nullptr;
-    int rc = evp_open(fft_in, out_dir, mix, modal, EVP_WRITE_FILES, &h);
+    // the files are only needed when the solve returns: VTK files are written in the background
+    int rc = open_solve(fft_in, out_dir, mix, modal, EVP_WRITE_FILES, true, &h);
     if (rc != 0) {
         if (report) { std::memset(report, 0, sizeof(*report)); report->status = rc; }
         return rc;
@@ -1834,6 +1891,13 @@ int evp_solve_file(const char* fft_in, const char* out_dir, int nthreads, const 
     while (true) {
         rc = evp_advance(h, 1, &done);
         if (rc != 0 || done == 0) break;
+    }
+    try {
+        h->s.wait_vtk();
+    } catch (SolveError& e) {
+        if (rc == 0) rc = fail(e.what(), e.code);
+    } catch (std::exception& e) {
+        if (rc == 0) rc = fail(e.what(), -1);
     }
     if (report) {
         evp_stats(h, report);
